@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Benchmark of the blockwise Gamma-SMC forward/backward scan on 1..N B200s.
+
+Metric: pair-site posteriors per second (pairs x sites / time), whole job.
+
+Workload (default ``chrom``): the chromosome-shape cohort -- 356 haplotypes
+(63,190 pairs) x 400,000 segregating sites, synthetic (seeded copying-mosaic
+genotypes; msprime is unavailable) -- decoded blockwise with
+core_block_sites = the API's auto choice on a B200 (32,768), flank_sites=2048,
+mean_only=True.  One step = one pass over the whole job.
+
+* ``value``: device-resident -- genotypes, tables and pair indices already in
+  HBM, the [n_sites x n_pairs] float32 output written to HBM (101 GB, far
+  larger than L2, so no flush is needed), timed with CUDA events.
+* ``e2e``: the same job through the public API with host buffers
+  (``FlowContext(G, positions, ...)`` + ``run_fb_blockwise`` into numpy), so
+  the H2D of the genotypes and the D2H of every posterior are inside the
+  timed region.
+* ``roofline``: the scan kernel's algorithmic bytes (4 B mean + 0.25 B of
+  genotype bits per pair-site) over its event-timed duration, against the
+  measured HBM copy bandwidth.
+* ``cpu_baseline``: the CPU oracle (a C++ restatement of the reference's scan,
+  OpenMP over pairs) on a bounded sample of the same workload.
+
+``--impl reference`` times the reference path's CPU implementation (the
+oracle port: the reference ships no CPU scan) on the host cores instead.
+Multi-GPU: one process per GPU (torchrun); each rank decodes its own cohort
+(weak scaling), no data-path collective.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "pair-site posteriors/sec"
+UNIT = "pair-sites/s"
+BYTES_MEAN_ONLY = 4.25      # 4 B fp32 mean + 2 genotype bits per pair-site
+BYTES_FULL_POSTERIOR = 12.25
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="chrom", choices=["chrom", "small"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    return ap.parse_args()
+
+
+def peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def workload(name, rank):
+    from gamma_smc_cu_b200 import synthetic
+    if name == "small":
+        G, pos = synthetic.cohort("small")
+        pairs = synthetic.all_pairs(G.shape[0])
+        return G, pos, pairs, G.shape[1], 0, "small: 40 haps x 2,127 sites x 780 pairs"
+    n, S, _, sp, sg = synthetic.COHORTS["chrom"]
+    span = synthetic.neutral_span(n, S)
+    pos = synthetic.positions_for(S, span, sp + 100 * rank)
+    G = synthetic.haplotypes(n, pos, sg + 100 * rank)
+    pairs = synthetic.all_pairs(n)
+    return G, pos, pairs, None, 2048, "chrom: 356 haps x 400,000 sites x 63,190 pairs"
+
+
+def cpu_baseline_sample(G, pos, pairs, core, flank, mu, rho, target_s=12.0):
+    """Time the CPU oracle on a bounded pair sample of the same job."""
+    from oracle import oracle as O
+    from gamma_smc_cu_b200._core import DEFAULT_FLOW_FIELD
+    threads = os.cpu_count() or 1
+    O.tables_for(DEFAULT_FLOW_FIELD, 1e4, mu, rho)
+    S = G.shape[1]
+    probe = pairs[:max(8, threads)]
+    t0 = time.perf_counter()
+    O.run_fb_blockwise(G, pos, [tuple(p) for p in probe], 1e4, mu, rho, DEFAULT_FLOW_FIELD,
+                       core, flank, True, False, threads)
+    dt = time.perf_counter() - t0
+    n_sample = int(min(len(pairs), max(len(probe), len(probe) * target_s / max(dt, 1e-3))))
+    sample = pairs[:n_sample]
+    t0 = time.perf_counter()
+    O.run_fb_blockwise(G, pos, [tuple(p) for p in sample], 1e4, mu, rho, DEFAULT_FLOW_FIELD,
+                       core, flank, True, False, threads)
+    dt = time.perf_counter() - t0
+    return {"value": n_sample * S / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n_sample} pairs x {S} sites, blockwise core={core} flank={flank}, "
+                      f"mean_only, {dt:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    G, pos, pairs, core, flank, desc = workload(args.workload, 0)
+    from gamma_smc_cu_b200.infer import _estimate_scaled_params, _recommend_core_block_size
+    from oracle import oracle as O
+    from gamma_smc_cu_b200._core import DEFAULT_FLOW_FIELD
+    S = G.shape[1]
+    if core is None:
+        core, _ = _recommend_core_block_size(S, len(pairs), True, flank, 178 * 10**9)
+    mu, rho = _estimate_scaled_params(G, pos, 1.25e-8, 1e-8, 1e4)
+    threads = os.cpu_count() or 1
+    O.tables_for(DEFAULT_FLOW_FIELD, 1e4, mu, rho)
+    probe = pairs[:max(8, threads)]
+    t0 = time.perf_counter()
+    O.run_fb_blockwise(G, pos, [tuple(p) for p in probe], 1e4, mu, rho, DEFAULT_FLOW_FIELD,
+                       core, flank, True, False, threads)
+    dt = time.perf_counter() - t0
+    n_sample = int(min(len(pairs), max(len(probe), len(probe) * 4.0 / max(dt, 1e-3))))
+    sample = [tuple(p) for p in pairs[:n_sample]]
+    for _ in range(args.warmup):
+        O.run_fb_blockwise(G, pos, sample, 1e4, mu, rho, DEFAULT_FLOW_FIELD, core, flank, True,
+                           False, threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.run_fb_blockwise(G, pos, sample, 1e4, mu, rho, DEFAULT_FLOW_FIELD, core, flank, True,
+                           False, threads)
+        times.append(time.perf_counter() - t0)
+    t = float(np.mean(times))
+    value = n_sample * S / t
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": desc, "core_block_sites": core, "flank_sites": flank,
+                       "mean_only": True},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{n_sample} pairs x {S} sites per step"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    import gamma_smc_cu_b200 as G200
+    from gamma_smc_cu_b200 import _core, _lib
+    from gamma_smc_cu_b200.infer import _estimate_scaled_params, _recommend_core_block_size
+
+    G, pos, pairs, core, flank, desc = workload(args.workload, rank)
+    S, P = G.shape[1], len(pairs)
+    free, _ = _core.cuda_mem_info()
+    if core is None:
+        core, _ = _recommend_core_block_size(S, P, True, flank, free)
+    mu, rho = _estimate_scaled_params(G, pos, 1.25e-8, 1e-8, 1e4)
+    ctx = _core.FlowContext(G, pos, 1e4, mu, rho, _core.DEFAULT_FLOW_FIELD, 0)
+    L = _lib.load()
+    dev = torch.device("cuda", local)
+    d_pi = torch.from_numpy(np.ascontiguousarray(pairs[:, 0])).to(dev)
+    d_pj = torch.from_numpy(np.ascontiguousarray(pairs[:, 1])).to(dev)
+    out = torch.empty((S, P), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        _lib.check(L.gsmc_run_fb_blockwise_device(
+            ctx.handle, d_pi.data_ptr(), d_pj.data_ptr(), P, core, flank, 0, out.data_ptr(),
+            None, None, None, None, P, 0, stream.cuda_stream))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ms = ctypes_double()
+    _lib.check(L.gsmc_ctx_timing_read(ctx.handle, None, None, None))
+    _lib.check(L.gsmc_ctx_timing(ctx.handle, 1))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t_ms = e0.elapsed_time(e1)
+    import ctypes
+    kms = ctypes.c_double()
+    launches = ctypes.c_int64()
+    psites = ctypes.c_double()
+    _lib.check(L.gsmc_ctx_timing_read(ctx.handle, ctypes.byref(kms), ctypes.byref(launches),
+                                      ctypes.byref(psites)))
+    _lib.check(L.gsmc_ctx_timing(ctx.handle, 0))
+    if world > 1:
+        t = torch.tensor([t_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms = float(t.item())
+    ms_per_step = t_ms / args.steps
+    value = P * S * world / (t_ms / 1e3 / args.steps)
+    hbm, peak_kind = peaks()
+    achieved = psites.value * BYTES_MEAN_ONLY / (kms.value / 1e3) / 1e9
+    sample = out[::max(1, S // 64), ::max(1, P // 64)]
+    assert bool(torch.isfinite(sample).all()) and bool((sample > 0).all()), "bad posterior"
+    del out
+    torch.cuda.empty_cache()
+
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(G, pos, pairs, core, flank, args.e2e_steps)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(G, pos, pairs, core, flank, mu, rho)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": desc, "core_block_sites": int(core), "flank_sites": flank,
+                       "mean_only": True, "l2": "output 101 GB >> L2 (no flush needed)",
+                       "parallelism": f"pairs replicated per rank x{world} (weak)"},
+            "gpu_launches": int(launches.value),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None,
+                         "peak_kind": peak_kind, "kernel": "fb_scan_kernel<false,false>",
+                         "kernel_ms_per_step": kms.value / args.steps,
+                         "bytes_per_pair_site": BYTES_MEAN_ONLY},
+            "clocks": clk.summary(),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def ctypes_double():
+    import ctypes
+    return ctypes.c_double()
+
+
+def run_e2e(G, pos, pairs, core, flank, steps):
+    """Public API with host buffers: context (H2D genotypes), blockwise run,
+    D2H of every posterior into numpy."""
+    import psutil
+    from gamma_smc_cu_b200 import _core
+    from gamma_smc_cu_b200.infer import _estimate_scaled_params
+    S, P = G.shape[1], len(pairs)
+    avail = psutil.virtual_memory().available
+    sites = S
+    if 4.0 * S * P > 0.6 * avail:
+        sites = int(0.6 * avail / (4.0 * P))
+    Gs, ps = np.ascontiguousarray(G[:, :sites]), np.ascontiguousarray(pos[:sites])
+    mu, rho = _estimate_scaled_params(Gs, ps, 1.25e-8, 1e-8, 1e4)
+    plist = [tuple(p) for p in pairs.tolist()]
+
+    def once():
+        ctx = _core.FlowContext(Gs, ps, 1e4, mu, rho, _core.DEFAULT_FLOW_FIELD, 0)
+        r = ctx.run_fb_blockwise(plist, core_block_sites=core, flank_sites=flank,
+                                 pair_batch_size=P, max_streams=1, mean_only=True)
+        ctx.close()
+        return r
+
+    r = once()  # warm-up (tables built once per parameter set, as in the reference)
+    del r
+    times = []
+    for _ in range(max(1, steps)):
+        t0 = time.perf_counter()
+        r = once()
+        times.append(time.perf_counter() - t0)
+        del r
+    t = float(np.mean(times))
+    return {"value": P * sites / t, "unit": UNIT, "h2d_bytes_per_step": int(Gs.nbytes + ps.nbytes + 8 * P),
+            "d2h_bytes_per_step": int(4 * sites * P), "seconds_per_step": t, "sites": sites,
+            "steps": len(times)}
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,211 @@
+"""Python face of the CUDA library with the reference's ``_core`` names.
+
+``FlowContext``, ``cuda_mem_info``, ``set_device``, ``get_device``,
+``get_device_count``, ``bitpack`` and ``unpack`` keep the signatures, defaults,
+result dictionaries and error types of the reference's pybind11 module
+(src/bindings.cpp:3630-3652, 3687-3730) and call ``lib/libgsmc_b200.so``
+through its C ABI (include/gsmc_b200.h).  ``infer.py`` looks these names up
+on this module at call time, so tests can monkeypatch them.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import _lib
+from ._lib import GSMC_CI, GSMC_POSTERIOR, check, ptr
+
+DEFAULT_FLOW_FIELD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data",
+                                  "default_flow_field.txt")
+
+
+def cuda_mem_info():
+    """(free_bytes, total_bytes) of the current CUDA device."""
+    L = _lib.load()
+    f = ctypes.c_uint64()
+    t = ctypes.c_uint64()
+    check(L.gsmc_mem_info(ctypes.byref(f), ctypes.byref(t)))
+    return int(f.value), int(t.value)
+
+
+def get_device_count():
+    n = ctypes.c_int()
+    check(_lib.load().gsmc_get_device_count(ctypes.byref(n)))
+    return int(n.value)
+
+
+def set_device(device_id):
+    check(_lib.load().gsmc_set_device(int(device_id)))
+
+
+def get_device():
+    d = ctypes.c_int()
+    check(_lib.load().gsmc_get_device(ctypes.byref(d)))
+    return int(d.value)
+
+
+def bitpack(G):
+    """Pack haplotypes into uint64 words, [n, ceil(S/64)] (bit b of word w = site 64w+b)."""
+    G = np.ascontiguousarray(G, dtype=np.uint8)
+    if G.ndim != 2:
+        raise RuntimeError("G must be 2D (n x S)")
+    n, S = G.shape
+    out = np.zeros((n, (S + 63) // 64), np.uint64)
+    check(_lib.load().gsmc_bitpack(ptr(G, _lib.c_u8p), n, S, ptr(out, _lib.c_u64p)))
+    return out
+
+
+def unpack(packed, n, S):
+    packed = np.ascontiguousarray(packed, dtype=np.uint64)
+    out = np.zeros((int(n), int(S)), np.uint8)
+    check(_lib.load().gsmc_unpack(ptr(packed, _lib.c_u64p), int(n), int(S),
+                                  ptr(out, _lib.c_u8p)))
+    return out
+
+
+def _split_pairs(pairs):
+    """List of (i, j) (or an (P, 2) array) -> two contiguous int32 arrays."""
+    if isinstance(pairs, np.ndarray):
+        arr = np.asarray(pairs)
+        if arr.size == 0:
+            arr = arr.reshape(0, 2)
+        if arr.ndim != 2 or arr.shape[1] != 2:
+            raise TypeError("pairs must be a sequence of (i, j) pairs")
+        return (np.ascontiguousarray(arr[:, 0], np.int32),
+                np.ascontiguousarray(arr[:, 1], np.int32))
+    pi = np.fromiter((int(p[0]) for p in pairs), dtype=np.int32)
+    pj = np.fromiter((int(p[1]) for p in pairs), dtype=np.int32)
+    return pi, pj
+
+
+class FlowContext:
+    """Resident genotypes, positions and flow-field tables on the current GPU.
+
+    Same constructor and methods as the reference's ``_core.FlowContext``
+    (src/bindings.cpp:2445-3346); the flow field defaults to the bundled
+    ``data/default_flow_field.txt``.
+    """
+
+    def __init__(self, G, positions, Ne=10000.0, mu=1.25e-8, rho=1e-8,
+                 flow_field_path=DEFAULT_FLOW_FIELD, cache_steps=0):
+        L = _lib.load()
+        G = np.ascontiguousarray(G, dtype=np.uint8)
+        positions = np.ascontiguousarray(positions, dtype=np.float64)
+        if G.ndim != 2:
+            raise ValueError("G must be 2D (n_haplotypes x n_sites)")
+        n, S = G.shape
+        if positions.ndim != 1 or positions.shape[0] != S:
+            raise ValueError("positions length must match the number of sites in G")
+        h = ctypes.c_void_p()
+        check(L.gsmc_ctx_create(ptr(G, _lib.c_u8p), n, S, ptr(positions, _lib.c_f64p),
+                                float(Ne), float(mu), float(rho),
+                                os.fsencode(str(flow_field_path)), int(cache_steps),
+                                ctypes.byref(h)))
+        self._h = h
+        self._n = n
+        self._S = S
+        d = ctypes.c_int()
+        check(L.gsmc_ctx_info(h, ctypes.byref(d), None, None))
+        self._device = int(d.value)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib._lib is not None:
+            _lib._lib.gsmc_ctx_destroy(h)
+            self._h = None
+
+    def close(self):
+        self.__del__()
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def device_id(self):
+        return self._device
+
+    @property
+    def n_haps(self):
+        return self._n
+
+    @property
+    def n_sites(self):
+        return self._S
+
+    def _outputs(self, rows, P, ci, posterior):
+        out = {"mean": np.empty((rows, P), np.float32)}
+        if ci:
+            out["lower"] = np.empty((rows, P), np.float32)
+            out["upper"] = np.empty((rows, P), np.float32)
+        if posterior:
+            out["posterior_alpha"] = np.empty((rows, P), np.float32)
+            out["posterior_beta"] = np.empty((rows, P), np.float32)
+        return out
+
+    @staticmethod
+    def _out_ptrs(out):
+        return [ptr(out.get(k), _lib.c_f32p) for k in
+                ("mean", "lower", "upper", "posterior_alpha", "posterior_beta")]
+
+    def run_fb(self, pairs, mean_only=True, return_posterior=False):
+        """Full-sequence forward-backward; dict of [n_sites, n_pairs] float32."""
+        pi, pj = _split_pairs(pairs)
+        P = len(pi)
+        if P == 0:
+            return self._outputs(self._S, 0, False, return_posterior)
+        ci = not mean_only
+        out = self._outputs(self._S, P, ci, return_posterior)
+        flags = (GSMC_CI if ci else 0) | (GSMC_POSTERIOR if return_posterior else 0)
+        check(_lib.load().gsmc_run_fb(self._h, ptr(pi, _lib.c_i32p), ptr(pj, _lib.c_i32p), P,
+                                      flags, *self._out_ptrs(out)))
+        return out
+
+    def run_fb_blockwise(self, pairs, core_block_sites=8192, flank_sites=2048,
+                         pair_batch_size=256, max_streams=1, mean_only=True,
+                         return_posterior=False):
+        """Blockwise forward-backward over flanked windows; adds ``blocks``."""
+        L = _lib.load()
+        # argument checks precede everything, as in src/bindings.cpp:3000-3016
+        if core_block_sites <= 0:
+            raise ValueError("core_block_sites must be positive.")
+        if flank_sites < 0:
+            raise ValueError("flank_sites must be non-negative.")
+        if pair_batch_size == 0 or pair_batch_size < -1:
+            raise ValueError("pair_batch_size must be positive or -1 for auto.")
+        if max_streams <= 0:
+            raise ValueError("max_streams must be positive.")
+        if return_posterior and max_streams > 1:
+            raise ValueError(
+                "return_posterior=True is currently only supported with max_streams=1. "
+                "Run blockwise posterior decoding in single-stream mode.")
+        pi, pj = _split_pairs(pairs)
+        P = len(pi)
+        nb = ctypes.c_int64()
+        check(L.gsmc_block_count(self._S, int(core_block_sites), ctypes.byref(nb)))
+        blocks = np.zeros((nb.value, 4), np.int32)
+        if P == 0:
+            out = self._outputs(self._S, 0, False, return_posterior)
+        elif nb.value == 0:
+            out = self._outputs(0, P, False, return_posterior)
+        else:
+            out = self._outputs(self._S, P, not mean_only, return_posterior)
+        flags = (GSMC_CI if not mean_only else 0) | (GSMC_POSTERIOR if return_posterior else 0)
+        if P == 0 or nb.value == 0:
+            flags = 0
+        check(L.gsmc_run_fb_blockwise(
+            self._h, ptr(pi, _lib.c_i32p), ptr(pj, _lib.c_i32p), P, int(core_block_sites),
+            int(flank_sites), int(pair_batch_size), int(max_streams), flags,
+            ptr(blocks, _lib.c_i32p), *self._out_ptrs(out)))
+        result = {"blocks": blocks}
+        result.update(out)
+        return result
+
+    def table_layer(self, table, layer):
+        """Debug: (m_grid, c_grid) [51, 50] of scan table 0..4 at a layer."""
+        buf = np.empty(2 * 2550, np.float32)
+        check(_lib.load().gsmc_ctx_table_layer(self._h, int(table), int(layer),
+                                               ptr(buf, _lib.c_f32p)))
+        return buf[:2550].reshape(51, 50), buf[2550:].reshape(51, 50)

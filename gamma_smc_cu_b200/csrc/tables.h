@@ -1,0 +1,49 @@
+// Flow-field grid, host table build and the scan's device table layout.
+#pragma once
+
+#include <cstddef>
+#include <vector>
+
+namespace gsmc {
+
+// 51 x 50 grid over log10 mean x log10 CV (include/gamma_smc_cu/flow_field.h:6-8).
+constexpr int kRows = 51;
+constexpr int kCols = 50;
+constexpr int kCells = kRows * kCols;
+// Interpolation cells: the lower-left corner index is clamped to rows < 50 and
+// columns < 49, so there are 50 x 49 distinct 2 x 2 patches.
+constexpr int kPatchRows = kRows - 1;
+constexpr int kPatchCols = kCols - 1;
+constexpr int kPatches = kPatchRows * kPatchCols;
+
+struct FlowField {
+  float u[kCells];
+  float v[kCells];
+  float m_lo, m_hi, c_lo, c_hi;  // log10 bounds read from the file header
+};
+
+// Host tables in the reference's layout, [n_steps][2550] each.
+enum HostTable {
+  kMissingMean = 0, kMissingCv, kHomMean, kHomCv,
+  kFwdHomMean, kFwdHomCv, kFwdHetMean, kFwdHetCv,
+  kBwdHomMean, kBwdHomCv, kBwdHetMean, kBwdHetCv,
+  kNumHostTables
+};
+
+struct HostLayers {
+  int n_steps = 0;
+  std::vector<float> t[kNumHostTables];
+};
+
+// Scan tables on the device: [kScanTables][n_steps][kPatches][8] floats.
+enum ScanTable { kScanFwdHom = 0, kScanFwdHet, kScanBwdHom, kScanBwdHet, kScanTables };
+
+int load_flow_field(const char* path, FlowField* ff, char* err, size_t err_len);
+void scaled_rates(double Ne, double mu, double rho, float* scaled_rho, float* scaled_mu);
+void build_layers(const FlowField& ff, int n_steps, float scaled_rho, float scaled_mu,
+                  int threads, HostLayers* out);
+void pack_patches(const float* m, const float* c, float* dst);
+void build_scan_layout(const HostLayers& h, std::vector<float>* site,
+                       std::vector<float>* chunk, int threads);
+
+}  // namespace gsmc

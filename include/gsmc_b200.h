@@ -1,0 +1,172 @@
+/*
+ * gsmc_b200.h - C ABI of the B200-native Gamma-SMC forward/backward scan.
+ *
+ * Plain C types only (no torch, no pybind11).  Every function returns a
+ * status: GSMC_OK (0) or a negative GSMC_E* code; gsmc_last_error() gives the
+ * message of the last failure on the calling thread.  Host pointers are
+ * ordinary pageable or pinned memory; "_device" entry points take device
+ * pointers and a cudaStream_t passed as void*.
+ *
+ * Output arrays are site-major: element (s, p) of an [n_sites x n_pairs]
+ * result is out[s * n_pairs + p], as in the reference (float32).
+ *
+ * Each entry point names the reference interface it replaces (paths are
+ * relative to the gamma_smc_cu source tree).
+ */
+#ifndef GSMC_B200_H
+#define GSMC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  GSMC_OK = 0,
+  GSMC_E_INVALID = -1,   /* bad argument: the reference raised ValueError   */
+  GSMC_E_CUDA = -2,      /* CUDA runtime error: reference RuntimeError       */
+  GSMC_E_IO = -3,        /* flow field could not be loaded                   */
+  GSMC_E_NOMEM = -4,     /* host or device allocation failed                 */
+  GSMC_E_TIMEOUT = -5    /* a bounded device wait gave up                    */
+};
+
+/* Output selection flags for the run_* calls. */
+enum {
+  GSMC_CI = 1,         /* write lower/upper Wilson-Hilferty 95% bounds (mean_only=False) */
+  GSMC_POSTERIOR = 2   /* write posterior_alpha/posterior_beta (return_posterior=True) */
+};
+
+typedef struct gsmc_ctx gsmc_ctx;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* gsmc_last_error(void);
+
+/* Library version string. */
+const char* gsmc_version(void);
+
+/* cudaMemGetInfo on the current device.
+ * Replaces _core.cuda_mem_info (src/bindings.cpp:3646-3652). */
+int gsmc_mem_info(uint64_t* free_bytes, uint64_t* total_bytes);
+
+/* Replace _core.get_device_count / set_device / get_device
+ * (src/bindings.cpp:3630-3644). */
+int gsmc_get_device_count(int* count);
+int gsmc_set_device(int device);
+int gsmc_get_device(int* device);
+
+/*
+ * Create a context on the current device: loads the flow field, builds or
+ * reuses the multi-step tables for (Ne, mu, rho, cache_steps), uploads and
+ * bit-packs the genotypes, uploads the positions.
+ *   G          [n_haps x n_sites] uint8, row-major (bit 0 of each byte is used)
+ *   positions  [n_sites] float64 site coordinates
+ *   cache_steps <= 0 selects 1000.
+ * Replaces FlowContext::FlowContext (src/bindings.cpp:2552-2670) together with
+ * ensure_flow_field / ensure_cache (src/bindings.cpp:2002-2157) and
+ * bitpack_genotypes_gpu (src/kernels/bitpack.cu:32-38).  Tables are owned per
+ * parameter set and reference-counted, never freed under a live context.
+ */
+int gsmc_ctx_create(const uint8_t* G, int64_t n_haps, int64_t n_sites,
+                    const double* positions, double Ne, double mu, double rho,
+                    const char* flow_field_path, int cache_steps,
+                    gsmc_ctx** out);
+
+/* Release a context (FlowContext::~FlowContext, src/bindings.cpp:2672-2677). */
+int gsmc_ctx_destroy(gsmc_ctx* ctx);
+
+/* Properties device_id / n_haps / n_sites (src/bindings.cpp:3727-3730). */
+int gsmc_ctx_info(const gsmc_ctx* ctx, int* device, int64_t* n_haps,
+                  int64_t* n_sites);
+
+/*
+ * Full-sequence forward/backward for n_pairs pairs (pair_i[p], pair_j[p]) into
+ * HOST arrays of [n_sites x n_pairs] float32.  mean is required; lower/upper
+ * are written when flags has GSMC_CI, alpha/beta when flags has
+ * GSMC_POSTERIOR (others may be NULL).  Pair indices outside [0, n_haps) are
+ * rejected with GSMC_E_INVALID.
+ * Replaces FlowContext::run_fb (src/bindings.cpp:2897-2989) and
+ * gamma_smc_flow_cached_fb_gpu (src/kernels/gamma_smc_flow.cu:844-903).
+ */
+int gsmc_run_fb(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j,
+                int64_t n_pairs, int flags, float* mean, float* lower,
+                float* upper, float* alpha, float* beta);
+
+/* Number of windows make_block_windows yields for (n_sites, core_block_sites). */
+int gsmc_block_count(int64_t n_sites, int64_t core_block_sites, int64_t* n_blocks);
+
+/*
+ * Blockwise forward/backward into HOST arrays of [n_sites x n_pairs] float32.
+ * Windows are (core_start, core_stop, padded_start, padded_stop) with padded =
+ * core +/- flank_sites clamped to [0, n_sites); each padded window restarts the
+ * scan and only its core rows are kept.  blocks_out receives n_blocks x 4 int32
+ * rows (size it with gsmc_block_count).  pair_batch_size (-1 = auto) caps the
+ * pairs per launch; max_streams > 1 overlaps windows; neither changes values.
+ * Replaces FlowContext::run_fb_blockwise (src/bindings.cpp:2991-3345) and the
+ * block kernels it launches (src/kernels/gamma_smc_flow.cu:618-669, 762-997).
+ */
+int gsmc_run_fb_blockwise(gsmc_ctx* ctx, const int32_t* pair_i,
+                          const int32_t* pair_j, int64_t n_pairs,
+                          int64_t core_block_sites, int64_t flank_sites,
+                          int64_t pair_batch_size, int max_streams, int flags,
+                          int32_t* blocks_out, float* mean, float* lower,
+                          float* upper, float* alpha, float* beta);
+
+/*
+ * Device-resident blockwise forward/backward: pair_i/pair_j and all outputs
+ * are DEVICE pointers; outputs are [n_sites x ld_out] float32 with pair p of
+ * this call written at column out_col0 + p.  core_block_sites >= n_sites with
+ * flank_sites = 0 is the full-sequence run_fb.  Work is enqueued on `stream`
+ * (a cudaStream_t, NULL = legacy default stream); scratch comes from the
+ * context's pool.  Returns after enqueueing; the caller synchronises.
+ * Same semantics as gsmc_run_fb_blockwise; no reference counterpart (the
+ * reference only offers host outputs).
+ */
+int gsmc_run_fb_blockwise_device(gsmc_ctx* ctx, const int32_t* d_pair_i,
+                                 const int32_t* d_pair_j, int64_t n_pairs,
+                                 int64_t core_block_sites, int64_t flank_sites,
+                                 int flags, float* d_mean, float* d_lower,
+                                 float* d_upper, float* d_alpha, float* d_beta,
+                                 int64_t ld_out, int64_t out_col0, void* stream);
+
+/* Bytes of device scratch the context currently holds (forward-state pool). */
+int gsmc_ctx_scratch_bytes(const gsmc_ctx* ctx, uint64_t* bytes);
+
+/*
+ * Kernel timing for measurement: while enabled, every scan launch of this
+ * context is bracketed by CUDA events on the stream it is launched on.
+ * gsmc_ctx_timing_read synchronises those events and returns the summed
+ * kernel milliseconds, the number of launches and the pair-sites (pairs x
+ * core sites) they produced since the last read, then resets the counters.
+ * No reference counterpart.
+ */
+int gsmc_ctx_timing(gsmc_ctx* ctx, int enable);
+int gsmc_ctx_timing_read(gsmc_ctx* ctx, double* kernel_ms, int64_t* launches,
+                         double* pair_sites);
+
+/*
+ * Bit-pack genotypes on the device: packed[h * n_words + w] bit b =
+ * G[h][64w + b] & 1, n_words = ceil(n_sites / 64); host in, host out.
+ * Replaces _core.bitpack / bitpack_kernel (src/kernels/bitpack.cu:11-38).
+ */
+int gsmc_bitpack(const uint8_t* G, int64_t n_haps, int64_t n_sites,
+                 uint64_t* packed);
+
+/* Inverse of gsmc_bitpack (_core.unpack, src/kernels/bitpack.cu:43-60). */
+int gsmc_unpack(const uint64_t* packed, int64_t n_haps, int64_t n_sites,
+                uint8_t* G);
+
+/*
+ * Copy the context's scan tables for one layer back to the host, for tests:
+ * table 0..4 = fwd_hom, fwd_het, bwd_hom, bwd_het, chunk; out receives
+ * 2 x 2550 floats (log10 mean grid, then log10 CV grid) of that layer.
+ * No reference counterpart (debug view of FlowFieldDeviceCacheView).
+ */
+int gsmc_ctx_table_layer(const gsmc_ctx* ctx, int table, int layer, float* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GSMC_B200_H */

@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="chrom", choices=["chrom", "small"])
+    ap.add_argument("--workload", default="chrom", choices=["chrom", "small", "chromprof"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
@@ -129,6 +129,13 @@ def workload(name, rank):
         G, pos = synthetic.cohort("small")
         pairs = synthetic.all_pairs(G.shape[0])
         return G, pos, pairs, G.shape[1], 0, "small: 40 haps x 2,127 sites x 780 pairs"
+    if name == "chromprof":
+        # profiling case with the chrom launch shape (all 63,190 pairs, several
+        # windows per launch) on 6,144 sites: core 2048, flank 1024 -> 3 windows,
+        # 1.55 GB output (> L2) + 3.1 GB forward states
+        G, pos = synthetic.cohort("chrom", n_sites=6144)
+        pairs = synthetic.all_pairs(G.shape[0])
+        return G, pos, pairs, 2048, 1024, "chromprof: 356 haps x 6,144 sites x 63,190 pairs"
     n, S, _, sp, sg = synthetic.COHORTS["chrom"]
     span = synthetic.neutral_span(n, S)
     pos = synthetic.positions_for(S, span, sp + 100 * rank)

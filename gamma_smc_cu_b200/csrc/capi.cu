@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -15,6 +16,7 @@
 #include <vector>
 
 #include "gsmc_b200.h"
+#include "hostcopy.h"
 #include "scan.h"
 #include "tables.h"
 
@@ -136,21 +138,28 @@ std::vector<Block> make_windows(int64_t S, int64_t core, int64_t flank) {
 
 }  // namespace
 
+
 struct gsmc_ctx {
   int device = 0;
   int64_t n_haps = 0, n_sites = 0, n_groups = 0;
   float ne = 0.0f;
   ulonglong2* geno = nullptr;
-  SiteCode* code = nullptr;
+  SiteCode* code = nullptr;  // points one past the leading pad entry
   TableSet* tables = nullptr;
-  // forward-state pool and pair-index buffer, grown on demand
-  void* pool = nullptr;
-  size_t pool_bytes = 0;
-  int32_t* pairs = nullptr;
-  int64_t pairs_cap = 0;
-  float* stage = nullptr;  // device staging of host-bound outputs
-  size_t stage_bytes = 0;
+  int pairs_per_thread = 1;  // independent chains per thread in the scan kernel
   cudaStream_t stream = nullptr;
+  // scratch, grown on demand and kept for the context's lifetime
+  void* pool = nullptr;  // forward-state slots of the persistent CTAs
+  size_t pool_bytes = 0;
+  int32_t* pairs = nullptr;  // host-path pair indices: [pi | pj]
+  int64_t pairs_cap = 0;
+  float* stage = nullptr;  // host-path output stage: two halves
+  size_t stage_bytes = 0;
+  Task* tasks[2] = {nullptr, nullptr};  // task lists of alternating launches
+  int64_t tasks_cap[2] = {0, 0};
+  int* counters = nullptr;  // work counter of each task list
+  cudaEvent_t stage_free[2] = {nullptr, nullptr};
+  cudaEvent_t launch_done[2] = {nullptr, nullptr};
   // measurement: events around scan launches while timing is on
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
@@ -160,46 +169,14 @@ struct gsmc_ctx {
 
 namespace {
 
-// Launch the scan, bracketed by events on `stream` when timing is enabled.
-cudaError_t launch_counted(gsmc_ctx* ctx, const ScanArgs& a, bool ci, bool post,
-                           cudaStream_t stream) {
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (ctx->timing) {
-    cudaError_t e = cudaEventCreate(&e0);
-    if (e == cudaSuccess) e = cudaEventCreate(&e1);
-    if (e == cudaSuccess) e = cudaEventRecord(e0, stream);
-    if (e != cudaSuccess) return e;
-  }
-  cudaError_t e = launch_scan(a, ci, post, stream);
-  if (e != cudaSuccess) return e;
-  ctx->launches++;
-  for (int i = 0; i < a.n_windows; ++i)
-    ctx->pair_sites += (double)a.n_pairs * (double)(a.win[i].ce - a.win[i].cs);
-  if (ctx->timing) {
-    e = cudaEventRecord(e1, stream);
-    if (e != cudaSuccess) return e;
-    ctx->events.emplace_back(e0, e1);
-  }
-  return cudaSuccess;
-}
-
-int ensure_pool(gsmc_ctx* ctx, size_t bytes) {
-  if (bytes <= ctx->pool_bytes) return GSMC_OK;
-  if (ctx->pool) cudaFree(ctx->pool);
-  ctx->pool = nullptr;
-  ctx->pool_bytes = 0;
-  CUDA_TRY(cudaMalloc(&ctx->pool, bytes));
-  ctx->pool_bytes = bytes;
-  return GSMC_OK;
-}
-
-int ensure_stage(gsmc_ctx* ctx, size_t bytes) {
-  if (bytes <= ctx->stage_bytes) return GSMC_OK;
-  if (ctx->stage) cudaFree(ctx->stage);
-  ctx->stage = nullptr;
-  ctx->stage_bytes = 0;
-  CUDA_TRY(cudaMalloc(&ctx->stage, bytes));
-  ctx->stage_bytes = bytes;
+template <class T>
+int ensure_buffer(T** buf, size_t* cap_bytes, size_t bytes) {
+  if (bytes <= *cap_bytes) return GSMC_OK;
+  if (*buf) cudaFree(*buf);
+  *buf = nullptr;
+  *cap_bytes = 0;
+  CUDA_TRY(cudaMalloc(buf, bytes));
+  *cap_bytes = bytes;
   return GSMC_OK;
 }
 
@@ -223,21 +200,12 @@ int upload_pairs(gsmc_ctx* ctx, const int32_t* pi, const int32_t* pj, int64_t P)
   return GSMC_OK;
 }
 
-ScanArgs base_args(const gsmc_ctx* ctx) {
-  ScanArgs a;
-  std::memset(&a, 0, sizeof(a));
-  a.geno = ctx->geno;
-  a.n_haps = ctx->n_haps;
-  a.code = ctx->code;
-  a.site_tab = ctx->tables->site;
-  a.chunk_tab = ctx->tables->chunk;
-  a.L = ctx->tables->L;
-  a.unscale = 2.0f * ctx->ne;
-  return a;
-}
-
 int n_outputs(int flags) {
   return 1 + ((flags & GSMC_CI) ? 2 : 0) + ((flags & GSMC_POSTERIOR) ? 2 : 0);
+}
+
+int task_flags(int flags) {
+  return ((flags & GSMC_CI) ? kTaskCI : 0) | ((flags & GSMC_POSTERIOR) ? kTaskPosterior : 0);
 }
 
 size_t free_device_bytes() {
@@ -246,128 +214,224 @@ size_t free_device_bytes() {
   return f;
 }
 
-// Plan pair chunk and windows per launch so that `per_pair_site` bytes of
-// scratch per (pair, core site) fit the budget.
-void plan(int64_t P, int64_t core_max, size_t per_pair_site, size_t budget, int64_t n_blocks,
-          int64_t pair_cap, int64_t* chunk, int64_t* wins) {
-  const size_t per_pair_window = std::max<size_t>(1, per_pair_site * (size_t)std::max<int64_t>(core_max, 1));
-  int64_t c = std::min<int64_t>(P, pair_cap > 0 ? pair_cap : P);
-  while (c > 1 && per_pair_window * (size_t)c > budget) c = (c + 1) / 2;
-  c = std::max<int64_t>(c, 1);
-  int64_t w = (int64_t)(budget / (per_pair_window * (size_t)c));
-  w = std::max<int64_t>(1, std::min<int64_t>({w, n_blocks, (int64_t)kMaxWindows}));
-  *chunk = c;
-  *wins = w;
+int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Resident CTAs of the persistent kernel, optionally capped for experiments.
+int resident_ctas(const gsmc_ctx* ctx) {
+  int r = std::max(1, scan_resident_ctas(ctx->pairs_per_thread));
+  if (const char* env = std::getenv("GSMC_MAX_CTAS")) r = std::max(1, std::min(r, std::atoi(env)));
+  return r;
 }
 
-// Device outputs of one call: pointers to [n_sites x ld] arrays.
-struct DeviceOut {
-  float* o[5];
-  int64_t ld;
-  int64_t col0;
+// Where the outputs of one window go: element (s, pair j) at
+// out[k][off + (s - row0) * ldo + j].
+struct WindowOut {
+  float* out[5];
+  int64_t off;
+  int64_t ldo;
+  int64_t row0;
 };
 
-// Run windows for all pairs writing device outputs directly.
-int run_direct(gsmc_ctx* ctx, const int32_t* d_pi, const int32_t* d_pj, int64_t P,
-               const std::vector<Block>& blocks, int flags, const DeviceOut& out,
-               cudaStream_t stream) {
-  if (P == 0 || blocks.empty()) return GSMC_OK;
-  int64_t core_max = 0;
-  for (const Block& b : blocks) core_max = std::max(core_max, b.ce - b.cs);
-  const size_t budget = (size_t)(0.45 * (double)free_device_bytes()) + ctx->pool_bytes;
-  int64_t chunk, wins;
-  plan(P, core_max, sizeof(float2), budget, (int64_t)blocks.size(), -1, &chunk, &wins);
-  int rc = ensure_pool(ctx, (size_t)chunk * core_max * wins * sizeof(float2));
+// Append the tasks of one window for pairs [pair0, pair0 + n), pair tile by
+// pair tile; `col` is the output column of pair pair0.
+void add_window_tasks(const Block& b, int64_t pair0, int64_t n, int tile, const WindowOut& wo,
+                      int64_t col, int flags, float unscale, std::vector<Task>* tasks) {
+  for (int64_t j = 0; j < n; j += tile) {
+    Task t;
+    std::memset(&t, 0, sizeof(t));
+    t.ps = (int32_t)b.ps;
+    t.cs = (int32_t)b.cs;
+    t.ce = (int32_t)b.ce;
+    t.pe = (int32_t)b.pe;
+    t.pair_begin = (int32_t)(pair0 + j);
+    t.pair_count = (int32_t)std::min<int64_t>(tile, n - j);
+    t.out_row0 = (int32_t)wo.row0;
+    t.flags = flags;
+    t.out_off = wo.off + col + j;
+    t.ldo = wo.ldo;
+    for (int k = 0; k < 5; ++k) t.out[k] = wo.out[k];
+    t.unscale = unscale;
+    tasks->push_back(t);
+  }
+}
+
+// Upload a task list into buffer `which` and launch the persistent scan with
+// up to `grid` CTAs over it; forward-state slots of slot_rows sites.
+int launch_tasks(gsmc_ctx* ctx, const std::vector<Task>& tasks, int which, const int32_t* d_pi,
+                 const int32_t* d_pj, int64_t slot_rows, int grid, cudaStream_t stream) {
+  if (tasks.empty()) return GSMC_OK;
+  size_t cap = (size_t)ctx->tasks_cap[which] * sizeof(Task);
+  int rc = ensure_buffer(&ctx->tasks[which], &cap, tasks.size() * sizeof(Task));
   if (rc) return rc;
-  ScanArgs a = base_args(ctx);
+  ctx->tasks_cap[which] = (int64_t)(cap / sizeof(Task));
+  CUDA_TRY(cudaMemcpyAsync(ctx->tasks[which], tasks.data(), tasks.size() * sizeof(Task),
+                           cudaMemcpyHostToDevice, stream));
+  CUDA_TRY(cudaMemsetAsync(ctx->counters + which, 0, sizeof(int), stream));
+  ScanArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.geno = ctx->geno;
+  a.n_haps = ctx->n_haps;
+  a.code = ctx->code;
+  a.site_tab = ctx->tables->site;
+  a.chunk_tab = ctx->tables->chunk;
+  a.L = ctx->tables->L;
+  a.pi = d_pi;
+  a.pj = d_pj;
+  a.tasks = ctx->tasks[which];
+  a.n_tasks = (int)tasks.size();
+  a.next_task = ctx->counters + which;
   a.fwd = static_cast<float2*>(ctx->pool);
-  a.mean = out.o[0];
-  a.lower = out.o[1];
-  a.upper = out.o[2];
-  a.alpha = out.o[3];
-  a.beta = out.o[4];
-  a.ldo = out.ld;
-  const bool ci = flags & GSMC_CI, post = flags & GSMC_POSTERIOR;
-  for (int64_t off = 0; off < P; off += chunk) {
-    const int64_t n = std::min(chunk, P - off);
-    a.pi = d_pi + off;
-    a.pj = d_pj + off;
-    a.n_pairs = n;
-    a.col0 = out.col0 + off;
-    for (size_t b0 = 0; b0 < blocks.size(); b0 += wins) {
-      const int nw = (int)std::min<int64_t>(wins, (int64_t)blocks.size() - (int64_t)b0);
-      a.n_windows = nw;
-      for (int i = 0; i < nw; ++i) {
-        const Block& b = blocks[b0 + i];
-        a.win[i] = Window{b.ps, b.cs, b.ce, b.pe, (int64_t)i * core_max * n, 0, 0};
-      }
-      CUDA_TRY(launch_counted(ctx, a, ci, post, stream));
-    }
+  a.slot_rows = slot_rows;
+  grid = (int)std::min<int64_t>(grid, (int64_t)tasks.size());
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (ctx->timing) {
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    CUDA_TRY(cudaEventRecord(e0, stream));
+  }
+  CUDA_TRY(launch_scan(a, grid, ctx->pairs_per_thread, stream));
+  ctx->launches++;
+  for (const Task& t : tasks) ctx->pair_sites += (double)t.pair_count * (double)(t.ce - t.cs);
+  if (ctx->timing) {
+    CUDA_TRY(cudaEventRecord(e1, stream));
+    ctx->events.emplace_back(e0, e1);
   }
   return GSMC_OK;
 }
 
-// Run windows writing HOST outputs: each launch writes window cores into a
-// device stage, copied out with one 2-D copy per output and window.
+int64_t max_core(const std::vector<Block>& blocks) {
+  int64_t m = 0;
+  for (const Block& b : blocks) m = std::max(m, b.ce - b.cs);
+  return m;
+}
+
+// Size the forward-state pool for up to `want` CTAs within `budget` bytes;
+// returns the CTA count it can hold (>= 1) or a negative status.
+int size_pool(gsmc_ctx* ctx, int64_t slot_rows, int want, size_t budget, int* grid) {
+  const size_t slot = (size_t)slot_rows * scan_tile_pairs(ctx->pairs_per_thread) * sizeof(float2);
+  int64_t g = std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)(budget / std::max<size_t>(slot, 1))));
+  int rc = ensure_buffer(reinterpret_cast<char**>(&ctx->pool), &ctx->pool_bytes, (size_t)g * slot);
+  if (rc) return rc;
+  *grid = (int)g;
+  return GSMC_OK;
+}
+
+// All windows x all pairs in one persistent launch, outputs written straight
+// into the caller's device arrays.
+int run_direct(gsmc_ctx* ctx, const int32_t* d_pi, const int32_t* d_pj, int64_t P,
+               const std::vector<Block>& blocks, int flags, float* const out[5], int64_t ld,
+               int64_t col0, cudaStream_t stream) {
+  if (P == 0 || blocks.empty()) return GSMC_OK;
+  const int tile = scan_tile_pairs(ctx->pairs_per_thread);
+  std::vector<Task> tasks;
+  tasks.reserve(blocks.size() * ceil_div(P, tile));
+  WindowOut wo{{out[0], out[1], out[2], out[3], out[4]}, 0, ld, 0};
+  for (const Block& b : blocks)
+    add_window_tasks(b, 0, P, tile, wo, col0, task_flags(flags), 2.0f * ctx->ne, &tasks);
+  const size_t budget = (size_t)(0.8 * (double)free_device_bytes()) + ctx->pool_bytes;
+  int grid = 0;
+  int rc = size_pool(ctx, max_core(blocks), resident_ctas(ctx), budget, &grid);
+  if (rc) return rc;
+  return launch_tasks(ctx, tasks, 0, d_pi, d_pj, max_core(blocks), grid, stream);
+}
+
+// Windows x pairs into HOST arrays.  Windows go in groups; each group's
+// launch writes its core rows into one half of a device stage while the
+// copier streams the previous group's half to the host.
 int run_to_host(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int64_t pair_cap,
                 int flags, float* const host[5]) {
   if (P == 0 || blocks.empty()) return GSMC_OK;
+  HostCopier* copier = HostCopier::for_current_device();
+  if (!copier) return fail(GSMC_E_CUDA, "CUDA error: no device for the host copier");
   const int nout = n_outputs(flags);
-  int64_t core_max = 0;
-  for (const Block& b : blocks) core_max = std::max(core_max, b.ce - b.cs);
-  const size_t budget =
-      (size_t)(0.8 * (double)free_device_bytes()) + ctx->pool_bytes + ctx->stage_bytes;
-  int64_t chunk, wins;
-  plan(P, core_max, sizeof(float2) + nout * sizeof(float), budget, (int64_t)blocks.size(),
-       pair_cap, &chunk, &wins);
-  int rc = ensure_pool(ctx, (size_t)chunk * core_max * wins * sizeof(float2));
+  const int tile = scan_tile_pairs(ctx->pairs_per_thread);
+  const int64_t core = max_core(blocks);
+  const int64_t nb = (int64_t)blocks.size();
+  const int resident = resident_ctas(ctx);
+  const size_t budget = (size_t)(0.75 * (double)free_device_bytes()) + ctx->pool_bytes +
+                        ctx->stage_bytes;
+  const size_t slot = (size_t)core * tile * sizeof(float2);
+  // pair chunk and windows per group: enough tasks per launch to fill the GPU
+  // twice, within the budget for pool + two stage halves
+  int64_t chunk = std::min<int64_t>(P, pair_cap > 0 ? pair_cap : P);
+  int64_t group = 1;
+  for (;;) {
+    group = std::min<int64_t>(nb, std::max<int64_t>(1, ceil_div(2 * resident, ceil_div(chunk, tile))));
+    for (;;) {
+      const int64_t want = std::min<int64_t>(resident, group * ceil_div(chunk, tile));
+      const size_t need = (size_t)want * slot + 2 * (size_t)group * core * chunk * nout * sizeof(float);
+      if (need <= budget || group == 1) break;
+      --group;
+    }
+    const int64_t want = std::min<int64_t>(resident, group * ceil_div(chunk, tile));
+    const size_t need = (size_t)want * slot + 2 * (size_t)group * core * chunk * nout * sizeof(float);
+    if (need <= budget || chunk <= tile) break;
+    chunk = std::max<int64_t>(tile, chunk / 2);
+  }
+  const size_t half = (size_t)group * core * chunk * nout;  // floats per stage half
+  int rc = ensure_buffer(&ctx->stage, &ctx->stage_bytes, 2 * half * sizeof(float));
   if (rc) return rc;
-  const size_t slot = (size_t)chunk * core_max;
-  rc = ensure_stage(ctx, slot * wins * nout * sizeof(float));
+  const size_t pool_budget = budget > 2 * half * sizeof(float) ? budget - 2 * half * sizeof(float) : slot;
+  int grid = 0;
+  rc = size_pool(ctx, core, resident, pool_budget, &grid);
   if (rc) return rc;
-  ScanArgs a = base_args(ctx);
-  a.fwd = static_cast<float2*>(ctx->pool);
-  float* dev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-  const int which[5] = {1, (flags & GSMC_CI) ? 1 : 0, (flags & GSMC_CI) ? 1 : 0,
-                        (flags & GSMC_POSTERIOR) ? 1 : 0, (flags & GSMC_POSTERIOR) ? 1 : 0};
-  int used = 0;
-  for (int k = 0; k < 5; ++k)
-    if (which[k]) dev[k] = ctx->stage + (size_t)(used++) * slot * wins;
-  a.mean = dev[0];
-  a.lower = dev[1];
-  a.upper = dev[2];
-  a.alpha = dev[3];
-  a.beta = dev[4];
-  const bool ci = flags & GSMC_CI, post = flags & GSMC_POSTERIOR;
-  for (int64_t off = 0; off < P; off += chunk) {
+  for (int i = 0; i < 2; ++i) {
+    if (!ctx->stage_free[i]) CUDA_TRY(cudaEventCreateWithFlags(&ctx->stage_free[i], cudaEventDisableTiming));
+    if (!ctx->launch_done[i]) CUDA_TRY(cudaEventCreateWithFlags(&ctx->launch_done[i], cudaEventDisableTiming));
+  }
+  const int32_t* d_pi = ctx->pairs;
+  const int32_t* d_pj = ctx->pairs + ctx->pairs_cap;
+  const int selected[5] = {1, (flags & GSMC_CI) ? 1 : 0, (flags & GSMC_CI) ? 1 : 0,
+                           (flags & GSMC_POSTERIOR) ? 1 : 0, (flags & GSMC_POSTERIOR) ? 1 : 0};
+  int64_t launch = 0;
+  int first_err = GSMC_OK;
+  for (int64_t off = 0; off < P && !first_err; off += chunk) {
     const int64_t n = std::min(chunk, P - off);
-    a.pi = ctx->pairs + off;
-    a.pj = ctx->pairs + ctx->pairs_cap + off;
-    a.n_pairs = n;
-    a.ldo = n;
-    a.col0 = 0;
-    for (size_t b0 = 0; b0 < blocks.size(); b0 += wins) {
-      const int nw = (int)std::min<int64_t>(wins, (int64_t)blocks.size() - (int64_t)b0);
-      a.n_windows = nw;
-      for (int i = 0; i < nw; ++i) {
-        const Block& b = blocks[b0 + i];
-        a.win[i] = Window{b.ps, b.cs, b.ce, b.pe, (int64_t)i * core_max * n,
-                          (int64_t)(i * slot), b.cs};
+    for (int64_t g0 = 0; g0 < nb && !first_err; g0 += group, ++launch) {
+      const int h = (int)(launch & 1);
+      const int64_t ng = std::min(group, nb - g0);
+      float* base = ctx->stage + (size_t)h * half;
+      if (launch >= 2) CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->stage_free[h], 0));
+      // stage layout of this half: [output k][window i][core rows][n pairs]
+      std::vector<Task> tasks;
+      for (int64_t i = 0; i < ng; ++i) {
+        const Block& b = blocks[g0 + i];
+        WindowOut wo;
+        int used = 0;
+        for (int k = 0; k < 5; ++k)
+          wo.out[k] = selected[k] ? base + (size_t)(used++) * group * core * n : nullptr;
+        wo.off = i * core * n;
+        wo.ldo = n;
+        wo.row0 = b.cs;
+        add_window_tasks(b, off, n, tile, wo, 0, task_flags(flags), 2.0f * ctx->ne, &tasks);
       }
-      CUDA_TRY(launch_counted(ctx, a, ci, post, ctx->stream));
-      for (int i = 0; i < nw; ++i) {
-        const Block& b = blocks[b0 + i];
+      rc = launch_tasks(ctx, tasks, h, d_pi, d_pj, core, grid, ctx->stream);
+      if (rc) return rc;
+      CUDA_TRY(cudaEventRecord(ctx->launch_done[h], ctx->stream));
+      for (int64_t i = 0; i < ng; ++i) {
+        const Block& b = blocks[g0 + i];
+        int used = 0;
         for (int k = 0; k < 5; ++k) {
-          if (!dev[k]) continue;
-          CUDA_TRY(cudaMemcpy2DAsync(host[k] + (size_t)b.cs * P + off, (size_t)P * sizeof(float),
-                                     dev[k] + (size_t)i * slot, (size_t)n * sizeof(float),
-                                     (size_t)n * sizeof(float), (size_t)(b.ce - b.cs),
-                                     cudaMemcpyDeviceToHost, ctx->stream));
+          if (!selected[k]) continue;
+          const float* src = base + (size_t)(used++) * group * core * n + (size_t)i * core * n;
+          const int e = copier->enqueue(host[k] + (size_t)b.cs * P + off, (size_t)P * sizeof(float),
+                                        src, (size_t)n * sizeof(float), (size_t)n * sizeof(float),
+                                        (size_t)(b.ce - b.cs), ctx->launch_done[h]);
+          if (e != cudaSuccess && !first_err)
+            first_err = fail(GSMC_E_CUDA, "CUDA error: %s (device to host copy)",
+                             cudaGetErrorString((cudaError_t)e));
         }
       }
-      CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+      const int e = copier->record_reads_done(ctx->stage_free[h]);
+      if (e != cudaSuccess && !first_err)
+        first_err = fail(GSMC_E_CUDA, "CUDA error: %s (copy event)", cudaGetErrorString((cudaError_t)e));
     }
   }
+  const int e = copier->drain();
+  if (first_err) return first_err;
+  if (e != cudaSuccess)
+    return fail(GSMC_E_CUDA, "CUDA error: %s (device to host copy)", cudaGetErrorString((cudaError_t)e));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return GSMC_OK;
 }
 
@@ -418,12 +482,18 @@ int gsmc_ctx_create(const uint8_t* G, int64_t n_haps, int64_t n_sites, const dou
     return fail(GSMC_E_INVALID, "null genotype or position array");
   if (!flow_field_path) return fail(GSMC_E_INVALID, "null flow field path");
   const int L = cache_steps <= 0 ? 1000 : cache_steps;  // src/bindings.cpp:2569-2572
+  if (L > kMaxCacheSteps)
+    return fail(GSMC_E_INVALID, "cache_steps must be at most %d", kMaxCacheSteps);
   auto ctx = std::make_unique<gsmc_ctx>();
   CUDA_TRY(cudaGetDevice(&ctx->device));
   ctx->n_haps = n_haps;
   ctx->n_sites = n_sites;
   ctx->ne = (float)Ne;
   ctx->n_groups = (n_sites + 127) / 128;
+  if (const char* env = std::getenv("GSMC_PAIRS_PER_THREAD")) {
+    const int v = std::atoi(env);
+    if (v == 1 || v == 2) ctx->pairs_per_thread = v;
+  }
   int rc = acquire_tables(ctx->device, flow_field_path, (float)Ne, (float)mu, (float)rho, L,
                           &ctx->tables);
   if (rc) return rc;
@@ -434,6 +504,7 @@ int gsmc_ctx_create(const uint8_t* G, int64_t n_haps, int64_t n_sites, const dou
     }
   } guard{&ctx};
   CUDA_TRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  CUDA_TRY(cudaMalloc(&ctx->counters, 2 * sizeof(int)));
   const size_t geno_bytes = (size_t)std::max<int64_t>(ctx->n_groups, 1) * std::max<int64_t>(n_haps, 1) * sizeof(ulonglong2);
   CUDA_TRY(cudaMalloc(&ctx->geno, geno_bytes));
   CUDA_TRY(cudaMemsetAsync(ctx->geno, 0, geno_bytes, ctx->stream));
@@ -447,16 +518,19 @@ int gsmc_ctx_create(const uint8_t* G, int64_t n_haps, int64_t n_sites, const dou
     cudaFree(dG);
     if (e != cudaSuccess) return fail(GSMC_E_CUDA, "CUDA error: %s (bitpack)", cudaGetErrorString(e));
   }
-  std::vector<SiteCode> codes((size_t)n_sites);
+  // Gap codes with one zero entry before site 0 and after the last site, so
+  // the kernel can prefetch the neighbouring site's code without a bound check.
+  std::vector<SiteCode> codes((size_t)n_sites + 2, SiteCode{0, 0});
   for (int64_t s = 0; s < n_sites; ++s) {
     const int k = seg_steps(s == 0 ? positions[0] + 1.0 : positions[s] - positions[s - 1]);
     const int chunks = (k - 1) / L;
-    codes[s] = SiteCode{k - chunks * L - 1, chunks};
+    codes[s + 1] = SiteCode{(k - chunks * L - 1) * kLayerF4, chunks};
   }
-  CUDA_TRY(cudaMalloc(&ctx->code, std::max<size_t>(1, codes.size()) * sizeof(SiteCode)));
-  if (n_sites > 0)
-    CUDA_TRY(cudaMemcpy(ctx->code, codes.data(), codes.size() * sizeof(SiteCode),
-                        cudaMemcpyHostToDevice));
+  SiteCode* code_base = nullptr;
+  CUDA_TRY(cudaMalloc(&code_base, codes.size() * sizeof(SiteCode)));
+  ctx->code = code_base + 1;
+  CUDA_TRY(cudaMemcpy(code_base, codes.data(), codes.size() * sizeof(SiteCode),
+                      cudaMemcpyHostToDevice));
   *out = ctx.release();
   return GSMC_OK;
 }
@@ -473,10 +547,16 @@ int gsmc_ctx_destroy(gsmc_ctx* ctx) {
     cudaEventDestroy(ev.second);
   }
   cudaFree(ctx->geno);
-  cudaFree(ctx->code);
+  if (ctx->code) cudaFree(ctx->code - 1);
   cudaFree(ctx->pool);
   cudaFree(ctx->pairs);
   cudaFree(ctx->stage);
+  cudaFree(ctx->counters);
+  for (int i = 0; i < 2; ++i) {
+    cudaFree(ctx->tasks[i]);
+    if (ctx->stage_free[i]) cudaEventDestroy(ctx->stage_free[i]);
+    if (ctx->launch_done[i]) cudaEventDestroy(ctx->launch_done[i]);
+  }
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   cudaSetDevice(prev);
   release_tables(ctx->tables);
@@ -535,6 +615,7 @@ int gsmc_block_count(int64_t n_sites, int64_t core, int64_t* n_blocks) {
   return GSMC_OK;
 }
 
+
 static int run_host_common(gsmc_ctx* ctx, const int32_t* pi, const int32_t* pj, int64_t P,
                            const std::vector<Block>& blocks, int64_t pair_cap, int flags,
                            float* mean, float* lower, float* upper, float* alpha,
@@ -589,6 +670,8 @@ int gsmc_run_fb_blockwise(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* p
       blocks_out[4 * b + 2] = (int32_t)blocks[b].ps;
       blocks_out[4 * b + 3] = (int32_t)blocks[b].pe;
     }
+  // Every window of every pair chunk runs on the persistent kernel regardless
+  // of max_streams: the copy engine already overlaps transfers with compute.
   return run_host_common(ctx, pair_i, pair_j, n_pairs, blocks, pair_batch_size, flags, mean,
                          lower, upper, alpha, beta);
 }
@@ -611,11 +694,11 @@ int gsmc_run_fb_blockwise_device(gsmc_ctx* ctx, const int32_t* d_pair_i, const i
     return fail(GSMC_E_INVALID, "null posterior output");
   CUDA_TRY(cudaSetDevice(ctx->device));
   const std::vector<Block> blocks = make_windows(ctx->n_sites, core_block_sites, flank_sites);
-  DeviceOut out{{d_mean, (flags & GSMC_CI) ? d_lower : nullptr, (flags & GSMC_CI) ? d_upper : nullptr,
-                 (flags & GSMC_POSTERIOR) ? d_alpha : nullptr,
-                 (flags & GSMC_POSTERIOR) ? d_beta : nullptr},
-                ld_out, out_col0};
-  return run_direct(ctx, d_pair_i, d_pair_j, n_pairs, blocks, flags, out,
+  float* const out[5] = {d_mean, (flags & GSMC_CI) ? d_lower : nullptr,
+                         (flags & GSMC_CI) ? d_upper : nullptr,
+                         (flags & GSMC_POSTERIOR) ? d_alpha : nullptr,
+                         (flags & GSMC_POSTERIOR) ? d_beta : nullptr};
+  return run_direct(ctx, d_pair_i, d_pair_j, n_pairs, blocks, flags, out, ld_out, out_col0,
                     static_cast<cudaStream_t>(stream));
 }
 
@@ -662,7 +745,7 @@ int gsmc_ctx_table_layer(const gsmc_ctx* ctx, int table, int layer, float* out) 
   if (table < 4 && (layer < 0 || layer >= L)) return fail(GSMC_E_INVALID, "layer out of range");
   std::vector<float> patches((size_t)kPatches * 8);
   const float4* src = table == 4 ? ctx->tables->chunk
-                                 : ctx->tables->site + ((size_t)table * L + layer) * kPatches * 2;
+                                 : ctx->tables->site + scan_layer_offset(table, layer, L);
   CUDA_TRY(cudaSetDevice(ctx->device));
   CUDA_TRY(cudaMemcpy(patches.data(), src, patches.size() * sizeof(float), cudaMemcpyDeviceToHost));
   // Rebuild the 51 x 50 grids from the patches' corners.

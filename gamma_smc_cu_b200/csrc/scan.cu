@@ -1,18 +1,22 @@
 // Fused Gamma-SMC forward/backward scan for sm_100a.
 //
-// One thread owns one (pair, window) and walks the window's sites: forward
-// from the padded start to the core end, storing its (m, c) state at core
-// sites, then backward from the padded end to the core start, combining with
-// the stored forward state and writing the posterior at core sites.  Sites are
-// shared by every pair, so the table layer chosen by the gap is the same for
-// all threads of the launch at a given site; only hom/het differs per pair.
+// Each thread owns NP pairs of one padded window and walks the window's sites:
+// forward from the padded start to the core end, storing the (m, c) state at
+// core sites, then backward from the padded end to the core start, combining
+// with the stored forward state and writing the posterior at core sites.
+// Sites are shared by every pair, so the gap code (table layer and number of
+// 1000-step chunks) is uniform across the launch; only hom/het differs per
+// pair.  The NP chains of a thread are independent, which gives the scheduler
+// NP-way instruction-level parallelism to hide the table-gather latency, and
+// the per-site uniform work (gap code, loop control) is shared by NP pairs.
 //
-// Table lookups read one 32-byte patch (four corners of m and of c) per step,
-// as two 16-byte read-only loads from a single sector; the patch tables stay
-// in L2 and the touched patches of the current layer in L1.  The arithmetic is
+// Table lookups read one 32-byte patch (four corners of m and of c) as two
+// 16-byte read-only loads from one sector; hom and het patches of a layer are
+// adjacent, so the het bit selects with one multiply-add.  The arithmetic is
 // the reference's cached FB (src/kernels/gamma_smc_flow.cu:112-131, 160-163,
-// 408-514, 567-609, 632-669, 678-754, 762-839) with every fused multiply-add
-// written explicitly, so results are bit-identical to it.
+// 408-514, 567-609, 632-669, 678-754, 762-839) with its fused multiply-adds
+// written explicitly; float->int conversions are replaced by exact integer
+// constructions, so results are bit-identical to it.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -33,123 +37,300 @@ constexpr float kCStep = (kCHi - kCLo) / (kCols - 1);
 constexpr float kMInv = 1.0f / kMStep;
 constexpr float kCInv = 1.0f / kCStep;
 
-// Bilinear lookup of (m, c) in one patch layer.
-__device__ __forceinline__ void patch_lookup(const float4* __restrict__ layer, float& m,
-                                             float& c) {
-  float fm = (m - kMLo) * kMInv;
-  float fc = (c - kCLo) * kCInv;
+// Bilinear lookup of (m, c) in one patch layer, identical to the reference's
+// clamp / truncate / keep-the-upper-cell interpolation.  Split in two so
+// independent work can be scheduled between the loads and their use.
+struct Fetch {
+  float4 a, b;  // m corners and c corners of the patch
+  float wm, wc;
+};
+
+__device__ __forceinline__ Fetch patch_fetch(const float4* __restrict__ layer, float m, float c) {
+  float fm = __fmul_rn(__fsub_rn(m, kMLo), kMInv);
+  float fc = __fmul_rn(__fsub_rn(c, kCLo), kCInv);
   fm = fmaxf(0.0f, fminf(fm, (float)(kRows - 1)));
   fc = fmaxf(0.0f, fminf(fc, (float)(kCols - 1)));
-  const int r = min((int)fm, kPatchRows - 1);
-  const int q = min((int)fc, kPatchCols - 1);
-  const float wm = fm - (float)r;
-  const float wc = fc - (float)q;
-  const float4* p = layer + 2 * (r * kPatchCols + q);
-  const float4 a = __ldg(p);      // m corners: (r,q) (r,q+1) (r+1,q) (r+1,q+1)
-  const float4 b = __ldg(p + 1);  // c corners
-  const float vc = 1.0f - wc, vm = 1.0f - wm;
-  m = __fmaf_rn(wm, __fmaf_rn(wc, a.w, vc * a.z), vm * __fmaf_rn(wc, a.y, vc * a.x));
-  c = __fmaf_rn(wm, __fmaf_rn(wc, b.w, vc * b.z), vm * __fmaf_rn(wc, b.y, vc * b.x));
+  // Lower-left corner: the reference truncates (fm >= 0, so floor) and moves
+  // an index that lands on the last row/column down by one.  floor(min(x,
+  // last - 0.5)) is both at once, and the weight stays x - corner.
+  const float rf = floorf(fminf(fm, (float)kPatchRows - 0.5f));
+  const float qf = floorf(fminf(fc, (float)kPatchCols - 0.5f));
+  Fetch f;
+  f.wm = __fsub_rn(fm, rf);
+  f.wc = __fsub_rn(fc, qf);
+  // rf * 49 + qf is an exact integer below 2450; adding 2^23 places it in the
+  // low mantissa bits, so the patch index needs no conversion instruction.
+  const int idx = __float_as_int(__fadd_rn(__fmaf_rn(rf, (float)kPatchCols, qf), 8388608.0f)) -
+                  0x4B000000;
+  const float4* p = layer + kPatchF4 * idx;
+  f.a = __ldg(p);      // (r,q) (r,q+1) (r+1,q) (r+1,q+1)
+  f.b = __ldg(p + 1);
+  return f;
+}
+
+__device__ __forceinline__ void patch_interp(const Fetch& f, float& m, float& c) {
+  const float vc = __fsub_rn(1.0f, f.wc), vm = __fsub_rn(1.0f, f.wm);
+  m = __fmaf_rn(f.wm, __fmaf_rn(f.wc, f.a.w, __fmul_rn(vc, f.a.z)),
+                __fmul_rn(vm, __fmaf_rn(f.wc, f.a.y, __fmul_rn(vc, f.a.x))));
+  c = __fmaf_rn(f.wm, __fmaf_rn(f.wc, f.b.w, __fmul_rn(vc, f.b.z)),
+                __fmul_rn(vm, __fmaf_rn(f.wc, f.b.y, __fmul_rn(vc, f.b.x))));
+}
+
+__device__ __forceinline__ void patch_lookup(const float4* __restrict__ layer, float& m,
+                                             float& c) {
+  const Fetch f = patch_fetch(layer, m, c);
+  patch_interp(f, m, c);
 }
 
 // 10^x by the bit construction upstream gamma_smc uses (Schraudolph 1999,
 // "A fast, compact approximation of the exponential function"): the float
-// with bits trunc(C2 * x * ln10 + C1) (src/kernels/gamma_smc_flow.cu:112-121).
+// whose bits are trunc(C2 * (x * ln10) + C1) (src/kernels/gamma_smc_flow.cu:
+// 112-121).
 __device__ __forceinline__ float pow10_bits(float x) {
   const float kLn10 = 2.30258509299f;
   const float kC1 = 1064872507.1541044f;
   const float kC2 = 12102203.161561485f;
-  return __int_as_float(__float2int_rz(__fmaf_rn(kC2, x * kLn10, kC1)));
+  return __int_as_float(__float2int_rz(__fmaf_rn(kC2, __fmul_rn(x, kLn10), kC1)));
 }
 
-__device__ __forceinline__ bool het_bit(uint64_t lo, uint64_t hi, int64_t s) {
-  const uint64_t w = (s & 64) ? hi : lo;
-  return ((w >> (s & 63)) & 1ull) != 0;
+__device__ __forceinline__ uint64_t word_at(const ulonglong2* g, int64_t nh, int s) {
+  const ulonglong2 v = __ldg(g + (int64_t)(s >> 7) * nh);
+  return (s & 64) ? v.y : v.x;
 }
 
-template <bool CI, bool POST>
-__global__ void __launch_bounds__(kScanThreads) fb_scan_kernel(const ScanArgs a) {
-  const int64_t p = (int64_t)blockIdx.x * kScanThreads + threadIdx.x;
-  if (p >= a.n_pairs) return;
-  const Window w = a.win[blockIdx.y];
+// Posterior combine at one core site: forward state f, backward state (m, c)
+// (src/kernels/gamma_smc_flow.cu:708-734).
+__device__ __forceinline__ void combine_store(const Task& t, int64_t o, float2 f, float m, float c,
+                                              bool ci, bool post) {
+  const float ab = -2.0f * c;
+  const float ba = pow10_bits(ab), bb = pow10_bits(__fsub_rn(ab, m));
+  const float af = -2.0f * f.y;
+  const float fa = pow10_bits(af), fb = pow10_bits(__fsub_rn(af, f.x));
+  const float a_s = __fsub_rn(__fadd_rn(fa, ba), 1.0f);
+  const float b_s = __fsub_rn(__fadd_rn(fb, bb), 1.0f);
+  const float mg = __fmul_rn(__fdiv_rn(a_s, fmaxf(b_s, 1e-10f)), t.unscale);
+  t.out[0][o] = mg;
+  if (ci) {
+    // Wilson-Hilferty 95% bounds (src/kernels/gamma_smc_flow.cu:724-733).
+    const float inv9a = __frcp_rn(__fmul_rn(9.0f, fmaxf(a_s, 1.0f)));
+    const float sq = __fsqrt_rn(inv9a);
+    const float base = __fsub_rn(1.0f, inv9a);
+    const float lo = fmaxf(__fmaf_rn(-1.96f, sq, base), 0.0f);
+    const float up = __fmaf_rn(1.96f, sq, base);
+    t.out[1][o] = fmaxf(__fmul_rn(__fmul_rn(__fmul_rn(mg, lo), lo), lo), 0.0f);
+    t.out[2][o] = __fmul_rn(__fmul_rn(__fmul_rn(mg, up), up), up);
+  }
+  if (post) {
+    t.out[3][o] = a_s;
+    t.out[4][o] = b_s;
+  }
+}
+
+// Forward states are read back this many sites ahead of their use so the
+// DRAM latency of that stream is hidden behind the scan's own lookups.
+constexpr int kFwdPrefetch = 4;
+constexpr int kThreads = 128;
+
+// One task: this thread's NP pairs over the task's padded window.  The
+// forward states live in this CTA's slot, rows of kThreads * NP pairs.
+template <int NP>
+__device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, float2* slot) {
+  constexpr int kRow = kThreads * NP;
   const int64_t nh = a.n_haps;
-  const int32_t hi = a.pi[p], hj = a.pj[p];
-  // Device-side pair indices are not validated by the host: skip bad ones
-  // (their outputs are left untouched) instead of reading out of bounds.
-  if (hi < 0 || hi >= nh || hj < 0 || hj >= nh) return;
-  const ulonglong2* gi = a.geno + hi;
-  const ulonglong2* gj = a.geno + hj;
-  const size_t layer_sz = (size_t)kPatches * 2;
-  const size_t table_sz = layer_sz * a.L;
-  const float4* fwd_hom = a.site_tab + kScanFwdHom * table_sz;
-  const float4* fwd_het = a.site_tab + kScanFwdHet * table_sz;
-  const float4* bwd_hom = a.site_tab + kScanBwdHom * table_sz;
-  const float4* bwd_het = a.site_tab + kScanBwdHet * table_sz;
-  float2* fwd = a.fwd + w.fwd_off + p;
+  const int ps = t.ps, cs = t.cs, ce = t.ce, pe = t.pe;
+  const bool ci = (t.flags & kTaskCI) != 0, post = (t.flags & kTaskPosterior) != 0;
+  const int j0 = threadIdx.x;
+  if (j0 >= t.pair_count) return;
 
-  // Forward sweep: state starts at (0, 0); a window that does not start at
-  // site 0 enters its first site with a 1-bp step.
-  float m = 0.0f, c = 0.0f;
-  int64_t group = -1;
-  uint64_t x0 = 0, x1 = 0;
-  for (int64_t s = w.ps; s < w.ce; ++s) {
-    if ((s >> 7) != group) {
-      group = s >> 7;
-      const ulonglong2 u = __ldg(gi + group * nh);
-      const ulonglong2 v = __ldg(gj + group * nh);
-      x0 = u.x ^ v.x;
-      x1 = u.y ^ v.y;
+  const ulonglong2* gi[NP];
+  const ulonglong2* gj[NP];
+  bool live[NP];
+#pragma unroll
+  for (int k = 0; k < NP; ++k) {
+    const int j = j0 + k * kThreads;
+    int hi = 0, hj = 0;
+    live[k] = j < t.pair_count;
+    if (live[k]) {
+      hi = a.pi[t.pair_begin + j];
+      hj = a.pj[t.pair_begin + j];
+      // Device-side pair indices are not validated by the host: a bad pair is
+      // skipped (outputs untouched) instead of reading out of bounds.
+      if (hi < 0 || hi >= nh || hj < 0 || hj >= nh) {
+        live[k] = false;
+        hi = hj = 0;
+      }
     }
-    SiteCode sc = a.code[s];
-    if (s == w.ps && w.ps > 0) sc = SiteCode{0, 0};
-    for (int k = 0; k < sc.chunks; ++k) patch_lookup(a.chunk_tab, m, c);
-    patch_lookup((het_bit(x0, x1, s) ? fwd_het : fwd_hom) + (size_t)sc.layer * layer_sz, m, c);
-    if (s >= w.cs) fwd[(s - w.cs) * a.n_pairs] = make_float2(m, c);
+    gi[k] = a.geno + hi;
+    gj[k] = a.geno + hj;
+  }
+  // code[-1] and code[n_sites] exist (zero padding), so the one-site-ahead
+  // prefetches below never leave the array.
+  const SiteCode* __restrict__ code = a.code;
+  const float4* __restrict__ fwd_tab = a.site_tab;
+  const float4* __restrict__ bwd_tab = a.site_tab + (size_t)a.L * kLayerF4;
+  const float4* __restrict__ chunk = a.chunk_tab;
+
+  // ---- forward: [ps, ce); states stored for [cs, ce) ----
+  float m[NP], c[NP];
+  uint64_t x[NP];
+#pragma unroll
+  for (int k = 0; k < NP; ++k) {
+    m[k] = 0.0f;
+    c[k] = 0.0f;
+    x[k] = (word_at(gi[k], nh, ps) ^ word_at(gj[k], nh, ps)) >> (ps & 63);
+  }
+  float2* fp = slot + j0;
+  auto fwd_step = [&](int s, SiteCode sc) {
+    if ((s & 63) == 0 && s != ps) {
+#pragma unroll
+      for (int k = 0; k < NP; ++k) x[k] = word_at(gi[k], nh, s) ^ word_at(gj[k], nh, s);
+    }
+    if (sc.chunks) {
+      for (int u = 0; u < sc.chunks; ++u) {
+#pragma unroll
+        for (int k = 0; k < NP; ++k) patch_lookup(chunk, m[k], c[k]);
+      }
+    }
+    const float4* layer = fwd_tab + sc.layer;
+    Fetch f[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      const int het = (int)(x[k] & 1ull);
+      x[k] >>= 1;
+      f[k] = patch_fetch(layer + het * kHetF4, m[k], c[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < NP; ++k) patch_interp(f[k], m[k], c[k]);
+  };
+  int s = ps;
+  SiteCode nxt = code[s + 1];
+  // a window that does not start at site 0 enters its first site by 1 bp
+  fwd_step(s, ps > 0 ? SiteCode{0, 0} : code[s]);
+  if (s >= cs) {
+#pragma unroll
+    for (int k = 0; k < NP; ++k) fp[k * kThreads] = make_float2(m[k], c[k]);
+    fp += kRow;
+  }
+  for (++s; s < cs; ++s) {
+    const SiteCode sc = nxt;
+    nxt = code[s + 1];
+    fwd_step(s, sc);
+  }
+  for (; s < ce; ++s) {
+    const SiteCode sc = nxt;
+    nxt = code[s + 1];
+    fwd_step(s, sc);
+#pragma unroll
+    for (int k = 0; k < NP; ++k) fp[k * kThreads] = make_float2(m[k], c[k]);
+    fp += kRow;
   }
 
-  // Backward sweep with the posterior combine at core sites.
-  const float unscale = a.unscale;
-  m = 0.0f;
-  c = 0.0f;
-  group = -1;
-  for (int64_t s = w.pe - 1; s >= w.cs; --s) {
-    if (s < w.ce) {
-      const float2 f = fwd[(s - w.cs) * a.n_pairs];
-      const float ab = -2.0f * c;
-      const float ba = pow10_bits(ab), bb = pow10_bits(ab - m);
-      const float af = -2.0f * f.y;
-      const float fa = pow10_bits(af), fb = pow10_bits(af - f.x);
-      const float a_s = fa + ba - 1.0f;
-      const float b_s = fb + bb - 1.0f;
-      const float mg = __fdiv_rn(a_s, fmaxf(b_s, 1e-10f)) * unscale;
-      const int64_t o = w.out_off + (s - w.out_row0) * a.ldo + a.col0 + p;
-      a.mean[o] = mg;
-      if constexpr (CI) {
-        // Wilson-Hilferty 95% bounds (src/kernels/gamma_smc_flow.cu:724-733).
-        const float inv9a = __frcp_rn(9.0f * fmaxf(a_s, 1.0f));
-        const float sq = __fsqrt_rn(inv9a);
-        const float base = 1.0f - inv9a;
-        const float lo = fmaxf(__fmaf_rn(-1.96f, sq, base), 0.0f);
-        const float up = __fmaf_rn(1.96f, sq, base);
-        a.lower[o] = fmaxf(mg * lo * lo * lo, 0.0f);
-        a.upper[o] = mg * up * up * up;
-      }
-      if constexpr (POST) {
-        a.alpha[o] = a_s;
-        a.beta[o] = b_s;
+  // ---- backward: [pe-1 .. cs]; posterior at core sites ----
+#pragma unroll
+  for (int k = 0; k < NP; ++k) {
+    m[k] = 0.0f;
+    c[k] = 0.0f;
+    x[k] = (word_at(gi[k], nh, pe - 1) ^ word_at(gj[k], nh, pe - 1)) << (63 - ((pe - 1) & 63));
+  }
+  // Backward step at site s: the het/hom site table first, then any full
+  // 1000-bp chunks; split so the combine can run between fetch and finish.
+  auto bwd_fetch = [&](int s, SiteCode sc, Fetch* f) {
+    if ((s & 63) == 63 && s != pe - 1) {
+#pragma unroll
+      for (int k = 0; k < NP; ++k) x[k] = word_at(gi[k], nh, s) ^ word_at(gj[k], nh, s);
+    }
+    const float4* layer = bwd_tab + sc.layer;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      const int het = (int)(x[k] >> 63);
+      x[k] <<= 1;
+      f[k] = patch_fetch(layer + het * kHetF4, m[k], c[k]);
+    }
+  };
+  auto bwd_finish = [&](SiteCode sc, const Fetch* f) {
+#pragma unroll
+    for (int k = 0; k < NP; ++k) patch_interp(f[k], m[k], c[k]);
+    if (sc.chunks) {
+      for (int u = 0; u < sc.chunks; ++u) {
+#pragma unroll
+        for (int k = 0; k < NP; ++k) patch_lookup(chunk, m[k], c[k]);
       }
     }
-    if (s == w.cs) break;
-    if ((s >> 7) != group) {
-      group = s >> 7;
-      const ulonglong2 u = __ldg(gi + group * nh);
-      const ulonglong2 v = __ldg(gj + group * nh);
-      x0 = u.x ^ v.x;
-      x1 = u.y ^ v.y;
+  };
+  s = pe - 1;
+  nxt = code[s];
+  for (; s >= ce; --s) {
+    const SiteCode sc = nxt;
+    nxt = code[s - 1];
+    Fetch f[NP];
+    bwd_fetch(s, sc, f);
+    bwd_finish(sc, f);
+  }
+  // forward-state ring: q[i] holds the state of site s - i
+  const float2* fq = slot + (int64_t)(ce - 1 - cs) * kRow + j0;
+  float2 q[kFwdPrefetch][NP];
+#pragma unroll
+  for (int i = 0; i < kFwdPrefetch; ++i) {
+#pragma unroll
+    for (int k = 0; k < NP; ++k)
+      q[i][k] = (ce - 1 - i >= cs) ? fq[k * kThreads] : make_float2(0.0f, 0.0f);
+    fq -= kRow;
+  }
+  int64_t o = t.out_off + (int64_t)(ce - 1 - t.out_row0) * t.ldo + j0;
+  // unrolled by the ring depth so the ring rotation is register renaming
+#pragma unroll kFwdPrefetch
+  for (s = ce - 1; s >= cs; --s) {
+    float2 f[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) f[k] = q[0][k];
+#pragma unroll
+    for (int i = 0; i + 1 < kFwdPrefetch; ++i) {
+#pragma unroll
+      for (int k = 0; k < NP; ++k) q[i][k] = q[i + 1][k];
     }
-    const SiteCode sc = a.code[s];
-    patch_lookup((het_bit(x0, x1, s) ? bwd_het : bwd_hom) + (size_t)sc.layer * layer_sz, m, c);
-    for (int k = 0; k < sc.chunks; ++k) patch_lookup(a.chunk_tab, m, c);
+    const bool ahead = s - kFwdPrefetch >= cs;
+#pragma unroll
+    for (int k = 0; k < NP; ++k)
+      q[kFwdPrefetch - 1][k] = ahead ? fq[k * kThreads] : make_float2(0.0f, 0.0f);
+    fq -= kRow;
+    const SiteCode sc = nxt;
+    nxt = code[s - 1];
+    float mb[NP], cb[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      mb[k] = m[k];
+      cb[k] = c[k];
+    }
+    Fetch fe[NP];
+    const bool more = s > cs;
+    if (more) bwd_fetch(s, sc, fe);
+#pragma unroll
+    for (int k = 0; k < NP; ++k)
+      if (live[k]) combine_store(t, o + k * kThreads, f[k], mb[k], cb[k], ci, post);
+    o -= t.ldo;
+    if (more) bwd_finish(sc, fe);
+  }
+}
+
+// Persistent scan: each CTA takes tasks from a global counter until none are
+// left; its forward-state slot is reused task after task.
+template <int NP>
+__global__ void __launch_bounds__(kThreads, NP == 1 ? 8 : 4)
+    fb_scan_persistent(const ScanArgs a) {
+  // The task descriptor lives in shared memory: its fields are uniform across
+  // the CTA and read only where used, so they cost no registers.
+  __shared__ Task task;
+  __shared__ int task_id;
+  float2* slot = a.fwd + (int64_t)blockIdx.x * a.slot_rows * (kThreads * NP);
+  for (;;) {
+    __syncthreads();  // everyone is done with the previous task
+    if (threadIdx.x == 0) {
+      task_id = atomicAdd(a.next_task, 1);
+      if (task_id < a.n_tasks) task = a.tasks[task_id];
+    }
+    __syncthreads();
+    if (task_id >= a.n_tasks) break;
+    scan_task<NP>(a, task, slot);
   }
 }
 
@@ -183,17 +364,32 @@ __global__ void unpack_kernel(const uint64_t* __restrict__ packed, int64_t n, in
 
 }  // namespace
 
-cudaError_t launch_scan(const ScanArgs& args, bool ci, bool posterior, cudaStream_t stream) {
-  if (args.n_pairs <= 0 || args.n_windows <= 0) return cudaSuccess;
-  const dim3 grid((unsigned)((args.n_pairs + kScanThreads - 1) / kScanThreads),
-                  (unsigned)args.n_windows);
-  if (ci) {
-    if (posterior) fb_scan_kernel<true, true><<<grid, kScanThreads, 0, stream>>>(args);
-    else fb_scan_kernel<true, false><<<grid, kScanThreads, 0, stream>>>(args);
-  } else {
-    if (posterior) fb_scan_kernel<false, true><<<grid, kScanThreads, 0, stream>>>(args);
-    else fb_scan_kernel<false, false><<<grid, kScanThreads, 0, stream>>>(args);
-  }
+int scan_threads() { return kThreads; }
+
+int scan_tile_pairs(int pairs_per_thread) {
+  return kThreads * (pairs_per_thread == 2 ? 2 : 1);
+}
+
+int scan_resident_ctas(int pairs_per_thread) {
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  cudaError_t e = pairs_per_thread == 2
+                      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fb_scan_persistent<2>,
+                                                                      kThreads, 0)
+                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fb_scan_persistent<1>,
+                                                                      kThreads, 0);
+  if (e != cudaSuccess) return 0;
+  return sms * per_sm;
+}
+
+cudaError_t launch_scan(const ScanArgs& args, int grid, int pairs_per_thread,
+                        cudaStream_t stream) {
+  if (args.n_tasks <= 0 || grid <= 0) return cudaSuccess;
+  if (pairs_per_thread == 2)
+    fb_scan_persistent<2><<<grid, kThreads, 0, stream>>>(args);
+  else
+    fb_scan_persistent<1><<<grid, kThreads, 0, stream>>>(args);
   return cudaGetLastError();
 }
 

@@ -6,52 +6,63 @@
 
 namespace gsmc {
 
-constexpr int kScanThreads = 256;     // threads per CTA of the scan
-constexpr int kMaxWindows = 32;       // windows one scan launch can carry
-
 // Per-site gap code: the gap of k base pairs entering site s is applied as
-// `chunks` lookups in the last hom layer plus one lookup in site layer `layer`,
-// with k = chunks * L + layer + 1 (src/kernels/gamma_smc_flow.cu:471-514).
+// `chunks` lookups in the last hom layer plus one lookup in site layer
+// j = k - chunks * L - 1 (src/kernels/gamma_smc_flow.cu:471-514).  `layer` is
+// j's offset in float4 units (j * kLayerF4) within one direction's tables.
 struct SiteCode {
   int layer;
   int chunks;
 };
 
-// One padded window: forward over [ps, ce), backward over [pe-1 .. cs],
-// outputs for core rows [cs, ce).  Rows of the outputs of this window live at
-// out + out_off + (s - out_row0) * ldo + col0 + p.
-struct Window {
-  int64_t ps, cs, ce, pe;
-  int64_t fwd_off;   // element offset of this window's forward-state slot
+// Output selection of a task.
+enum TaskFlags { kTaskCI = 1, kTaskPosterior = 2 };
+
+// One unit of scan work: up to (threads per CTA x pairs per thread) pairs over
+// one padded window.  Forward over [ps, ce), backward over [pe-1 .. cs],
+// posterior at core rows [cs, ce).  Output element (s, pair j of the task) is
+// out[k][out_off + (s - out_row0) * ldo + j] for each selected output k
+// (0 mean, 1 lower, 2 upper, 3 alpha, 4 beta).
+struct Task {
+  int32_t ps, cs, ce, pe;
+  int32_t pair_begin;   // first pair (index into pi/pj)
+  int32_t pair_count;   // pairs in this task
+  int32_t out_row0;
+  int32_t flags;        // TaskFlags
   int64_t out_off;
-  int64_t out_row0;
+  int64_t ldo;
+  float* out[5];
+  float unscale;        // 2 * Ne of the task's job
+  int32_t pad;
 };
 
 struct ScanArgs {
   const ulonglong2* geno;   // [n_groups][n_haps]: 128 sites per entry, bit b of .x/.y = site 128g+b / 128g+64+b
   int64_t n_haps;
-  const SiteCode* code;     // [n_sites]
-  const float4* site_tab;   // [4][L][2450][2]
+  const SiteCode* code;     // [n_sites], with one zero entry before and after
+  const float4* site_tab;   // [2 directions][L][hom, het][2450][2]
   const float4* chunk_tab;  // [2450][2]
   int L;
   const int32_t* pi;
   const int32_t* pj;
-  int64_t n_pairs;          // pairs in this launch (also the forward-state row stride)
-  float2* fwd;              // forward states (m, c), slot rows of n_pairs
-  float* mean;
-  float* lower;
-  float* upper;
-  float* alpha;
-  float* beta;
-  int64_t ldo;
-  int64_t col0;
-  float unscale;            // 2 * Ne
-  int n_windows;
-  Window win[kMaxWindows];
+  const Task* tasks;
+  int n_tasks;
+  int* next_task;           // work counter, zero at launch
+  float2* fwd;              // per-CTA forward-state slots
+  int64_t slot_rows;        // sites per slot (max core length of the tasks)
 };
 
-// Launch the fused forward/backward scan over args.n_windows windows.
-cudaError_t launch_scan(const ScanArgs& args, bool ci, bool posterior, cudaStream_t stream);
+// Threads per CTA of the scan and the pairs one thread carries.
+int scan_threads();
+int scan_tile_pairs(int pairs_per_thread);
+
+// Resident CTAs of the persistent scan kernel on the current device.
+int scan_resident_ctas(int pairs_per_thread);
+
+// Launch the persistent scan over args.n_tasks tasks with `grid` CTAs; each
+// CTA owns forward-state slot blockIdx.x of slot_rows x tile pairs float2.
+cudaError_t launch_scan(const ScanArgs& args, int grid, int pairs_per_thread,
+                        cudaStream_t stream);
 
 // Pack [n_haps x n_sites] uint8 genotypes.  scan_layout: word-major 128-site
 // groups for the scan; otherwise the reference's row-major uint64 words.

@@ -304,7 +304,7 @@ void build_scan_layout(const HostLayers& h, std::vector<float>* site, std::vecto
       const int t = (int)(tl / L), k = (int)(tl % L);
       pack_patches(h.t[kSrc[t][0]].data() + (size_t)k * kCells,
                    h.t[kSrc[t][1]].data() + (size_t)k * kCells,
-                   site->data() + (size_t)tl * per_layer);
+                   site->data() + scan_layer_offset(t, k, L) * 4);
     }
   });
   chunk->assign(per_layer, 0.0f);

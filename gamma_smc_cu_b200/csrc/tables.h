@@ -35,8 +35,21 @@ struct HostLayers {
   std::vector<float> t[kNumHostTables];
 };
 
-// Scan tables on the device: [kScanTables][n_steps][kPatches][8] floats.
+// Scan tables on the device: [direction][n_steps][hom, het][kPatches][8]
+// floats, so the hom and het patches of one layer are adjacent and a pair's
+// het bit selects between them with one multiply-add.  Offsets below are in
+// float4 units (two per patch).
 enum ScanTable { kScanFwdHom = 0, kScanFwdHet, kScanBwdHom, kScanBwdHet, kScanTables };
+constexpr int kPatchF4 = 2;                         // float4 per patch
+constexpr int kHetF4 = kPatches * kPatchF4;         // hom -> het of one layer
+constexpr int kLayerF4 = 2 * kHetF4;                // one layer (hom + het)
+// Layer offsets are int32 float4 indices: cap the cache depth accordingly.
+constexpr int kMaxCacheSteps = 100000;
+
+inline size_t scan_layer_offset(int table, int layer, int L) {
+  const int dir = table / 2, het = table % 2;
+  return ((size_t)dir * L + layer) * kLayerF4 + (size_t)het * kHetF4;
+}
 
 int load_flow_field(const char* path, FlowField* ff, char* err, size_t err_len);
 void scaled_rates(double Ne, double mu, double rho, float* scaled_rho, float* scaled_mu);

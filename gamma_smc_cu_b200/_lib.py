@@ -13,7 +13,7 @@ import threading
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libgsmc_b200.so")
+LIB_PATH = os.environ.get("GSMC_LIB_PATH") or os.path.join(HERE, "lib", "libgsmc_b200.so")
 
 GSMC_OK = 0
 GSMC_E_INVALID = -1

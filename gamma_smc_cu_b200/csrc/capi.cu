@@ -144,7 +144,7 @@ struct gsmc_ctx {
   int64_t n_haps = 0, n_sites = 0, n_groups = 0;
   float ne = 0.0f;
   ulonglong2* geno = nullptr;
-  SiteCode* code = nullptr;  // points one past the leading pad entry
+  SiteCode* code = nullptr;  // site 0 of the code array (kCodePad entries before it)
   TableSet* tables = nullptr;
   int pairs_per_thread = 1;  // independent chains per thread in the scan kernel
   cudaStream_t stream = nullptr;
@@ -518,17 +518,17 @@ int gsmc_ctx_create(const uint8_t* G, int64_t n_haps, int64_t n_sites, const dou
     cudaFree(dG);
     if (e != cudaSuccess) return fail(GSMC_E_CUDA, "CUDA error: %s (bitpack)", cudaGetErrorString(e));
   }
-  // Gap codes with one zero entry before site 0 and after the last site, so
-  // the kernel can prefetch the neighbouring site's code without a bound check.
-  std::vector<SiteCode> codes((size_t)n_sites + 2, SiteCode{0, 0});
+  // Gap codes with two zero entries before site 0 and after the last site, so
+  // the kernel can prefetch the codes two sites ahead without a bound check.
+  std::vector<SiteCode> codes((size_t)n_sites + 2 * kCodePad, SiteCode{0, 0});
   for (int64_t s = 0; s < n_sites; ++s) {
     const int k = seg_steps(s == 0 ? positions[0] + 1.0 : positions[s] - positions[s - 1]);
     const int chunks = (k - 1) / L;
-    codes[s + 1] = SiteCode{(k - chunks * L - 1) * kLayerF4, chunks};
+    codes[s + kCodePad] = SiteCode{(k - chunks * L - 1) * kLayerF4, chunks};
   }
   SiteCode* code_base = nullptr;
   CUDA_TRY(cudaMalloc(&code_base, codes.size() * sizeof(SiteCode)));
-  ctx->code = code_base + 1;
+  ctx->code = code_base + kCodePad;
   CUDA_TRY(cudaMemcpy(code_base, codes.data(), codes.size() * sizeof(SiteCode),
                       cudaMemcpyHostToDevice));
   *out = ctx.release();
@@ -547,7 +547,7 @@ int gsmc_ctx_destroy(gsmc_ctx* ctx) {
     cudaEventDestroy(ev.second);
   }
   cudaFree(ctx->geno);
-  if (ctx->code) cudaFree(ctx->code - 1);
+  if (ctx->code) cudaFree(ctx->code - kCodePad);
   cudaFree(ctx->pool);
   cudaFree(ctx->pairs);
   cudaFree(ctx->stage);

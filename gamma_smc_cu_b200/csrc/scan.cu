@@ -1,22 +1,21 @@
 // Fused Gamma-SMC forward/backward scan for sm_100a.
 //
-// Each thread owns NP pairs of one padded window and walks the window's sites:
-// forward from the padded start to the core end, storing the (m, c) state at
-// core sites, then backward from the padded end to the core start, combining
-// with the stored forward state and writing the posterior at core sites.
-// Sites are shared by every pair, so the gap code (table layer and number of
-// 1000-step chunks) is uniform across the launch; only hom/het differs per
-// pair.  The NP chains of a thread are independent, which gives the scheduler
-// NP-way instruction-level parallelism to hide the table-gather latency, and
-// the per-site uniform work (gap code, loop control) is shared by NP pairs.
+// A persistent kernel: every CTA pulls tasks -- up to 128 (x NP) pairs over
+// one padded window -- from a device counter.  Each thread walks its pairs
+// over the window's sites: forward from the padded start to the core end,
+// storing the (m, c) state at core sites in the CTA's slot, then backward from
+// the padded end to the core start, combining with the stored forward state
+// and writing the posterior at core sites.  Sites are shared by every pair, so
+// the gap code (table layer and number of 1000-step chunks) is uniform across
+// a task; only hom/het differs per pair.  With NP > 1 a thread's chains are
+// independent (instruction-level parallelism) and share the per-site work.
 //
-// Table lookups read one 32-byte patch (four corners of m and of c) as two
-// 16-byte read-only loads from one sector; hom and het patches of a layer are
-// adjacent, so the het bit selects with one multiply-add.  The arithmetic is
-// the reference's cached FB (src/kernels/gamma_smc_flow.cu:112-131, 160-163,
+// Table lookups read one 32-byte patch (four corners of m and of c) with a
+// single 256-bit read-only load; hom and het patches of a layer are adjacent,
+// so the het bit selects with one multiply-add.  The arithmetic is the
+// reference's cached FB (src/kernels/gamma_smc_flow.cu:112-131, 160-163,
 // 408-514, 567-609, 632-669, 678-754, 762-839) with its fused multiply-adds
-// written explicitly; float->int conversions are replaced by exact integer
-// constructions, so results are bit-identical to it.
+// written explicitly, so results are bit-identical to it.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -43,7 +42,18 @@ constexpr float kCInv = 1.0f / kCStep;
 struct Fetch {
   float4 a, b;  // m corners and c corners of the patch
   float wm, wc;
+  int idx;      // patch index within the layer
 };
+
+// Hint the patch a pair will most likely read at its next site (same cell,
+// next site's layer, next site's hom/het half) into L1.
+__device__ __forceinline__ void prefetch_patch(const float4* p) {
+#ifdef GSMC_PREFETCH_NEXT
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+#else
+  (void)p;
+#endif
+}
 
 __device__ __forceinline__ Fetch patch_fetch(const float4* __restrict__ layer, float m, float c) {
   float fm = __fmul_rn(__fsub_rn(m, kMLo), kMInv);
@@ -62,9 +72,16 @@ __device__ __forceinline__ Fetch patch_fetch(const float4* __restrict__ layer, f
   // low mantissa bits, so the patch index needs no conversion instruction.
   const int idx = __float_as_int(__fadd_rn(__fmaf_rn(rf, (float)kPatchCols, qf), 8388608.0f)) -
                   0x4B000000;
+  // One 256-bit read-only load of the 32-byte patch: m corners (r,q) (r,q+1)
+  // (r+1,q) (r+1,q+1), then the c corners.  Patches are 32-byte aligned:
+  // table bases come from cudaMalloc and every layer, hom/het half and patch
+  // offset is a multiple of 32 bytes.
+  f.idx = idx;
   const float4* p = layer + kPatchF4 * idx;
-  f.a = __ldg(p);      // (r,q) (r,q+1) (r+1,q) (r+1,q+1)
-  f.b = __ldg(p + 1);
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(f.a.x), "=f"(f.a.y), "=f"(f.a.z), "=f"(f.a.w), "=f"(f.b.x), "=f"(f.b.y),
+        "=f"(f.b.z), "=f"(f.b.w)
+      : "l"(p));
   return f;
 }
 
@@ -109,7 +126,7 @@ __device__ __forceinline__ void combine_store(const Task& t, int64_t o, float2 f
   const float a_s = __fsub_rn(__fadd_rn(fa, ba), 1.0f);
   const float b_s = __fsub_rn(__fadd_rn(fb, bb), 1.0f);
   const float mg = __fmul_rn(__fdiv_rn(a_s, fmaxf(b_s, 1e-10f)), t.unscale);
-  t.out[0][o] = mg;
+  __stcs(t.out[0] + o, mg);
   if (ci) {
     // Wilson-Hilferty 95% bounds (src/kernels/gamma_smc_flow.cu:724-733).
     const float inv9a = __frcp_rn(__fmul_rn(9.0f, fmaxf(a_s, 1.0f)));
@@ -117,17 +134,19 @@ __device__ __forceinline__ void combine_store(const Task& t, int64_t o, float2 f
     const float base = __fsub_rn(1.0f, inv9a);
     const float lo = fmaxf(__fmaf_rn(-1.96f, sq, base), 0.0f);
     const float up = __fmaf_rn(1.96f, sq, base);
-    t.out[1][o] = fmaxf(__fmul_rn(__fmul_rn(__fmul_rn(mg, lo), lo), lo), 0.0f);
-    t.out[2][o] = __fmul_rn(__fmul_rn(__fmul_rn(mg, up), up), up);
+    __stcs(t.out[1] + o, fmaxf(__fmul_rn(__fmul_rn(__fmul_rn(mg, lo), lo), lo), 0.0f));
+    __stcs(t.out[2] + o, __fmul_rn(__fmul_rn(__fmul_rn(mg, up), up), up));
   }
   if (post) {
-    t.out[3][o] = a_s;
-    t.out[4][o] = b_s;
+    __stcs(t.out[3] + o, a_s);
+    __stcs(t.out[4] + o, b_s);
   }
 }
 
 // Forward states are read back this many sites ahead of their use so the
-// DRAM latency of that stream is hidden behind the scan's own lookups.
+// DRAM latency of that stream is hidden behind the scan's own lookups.  They
+// and the outputs are single-use streams: stored with evict-first (.cs) and
+// read with last-use (.lu) hints so they do not displace table patches.
 constexpr int kFwdPrefetch = 4;
 constexpr int kThreads = 128;
 
@@ -163,8 +182,8 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     gi[k] = a.geno + hi;
     gj[k] = a.geno + hj;
   }
-  // code[-1] and code[n_sites] exist (zero padding), so the one-site-ahead
-  // prefetches below never leave the array.
+  // code[-2..-1] and code[n_sites..n_sites+1] exist (zero padding), so the
+  // two-sites-ahead code prefetches below never leave the array.
   const SiteCode* __restrict__ code = a.code;
   const float4* __restrict__ fwd_tab = a.site_tab;
   const float4* __restrict__ bwd_tab = a.site_tab + (size_t)a.L * kLayerF4;
@@ -180,7 +199,9 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     x[k] = (word_at(gi[k], nh, ps) ^ word_at(gj[k], nh, ps)) >> (ps & 63);
   }
   float2* fp = slot + j0;
-  auto fwd_step = [&](int s, SiteCode sc) {
+  // Gap codes run two sites ahead: `cur` is this site's, `nx` the next one's
+  // (already in registers, so the next-site prefetch does not wait on it).
+  auto fwd_step = [&](int s, SiteCode sc, int next_layer) {
     if ((s & 63) == 0 && s != ps) {
 #pragma unroll
       for (int k = 0; k < NP; ++k) x[k] = word_at(gi[k], nh, s) ^ word_at(gj[k], nh, s);
@@ -198,30 +219,39 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
       const int het = (int)(x[k] & 1ull);
       x[k] >>= 1;
       f[k] = patch_fetch(layer + het * kHetF4, m[k], c[k]);
+      prefetch_patch(fwd_tab + next_layer + (int)(x[k] & 1ull) * kHetF4 + kPatchF4 * f[k].idx);
     }
 #pragma unroll
     for (int k = 0; k < NP; ++k) patch_interp(f[k], m[k], c[k]);
   };
   int s = ps;
-  SiteCode nxt = code[s + 1];
   // a window that does not start at site 0 enters its first site by 1 bp
-  fwd_step(s, ps > 0 ? SiteCode{0, 0} : code[s]);
+  SiteCode cur = ps > 0 ? SiteCode{0, 0} : code[s];
+  SiteCode nx = code[s + 1];
+  {
+    const SiteCode nx2 = code[s + 2];
+    fwd_step(s, cur, nx.layer);
+    cur = nx;
+    nx = nx2;
+  }
   if (s >= cs) {
 #pragma unroll
-    for (int k = 0; k < NP; ++k) fp[k * kThreads] = make_float2(m[k], c[k]);
+    for (int k = 0; k < NP; ++k) __stcs(fp + k * kThreads, make_float2(m[k], c[k]));
     fp += kRow;
   }
   for (++s; s < cs; ++s) {
-    const SiteCode sc = nxt;
-    nxt = code[s + 1];
-    fwd_step(s, sc);
+    const SiteCode nx2 = code[s + 2];
+    fwd_step(s, cur, nx.layer);
+    cur = nx;
+    nx = nx2;
   }
   for (; s < ce; ++s) {
-    const SiteCode sc = nxt;
-    nxt = code[s + 1];
-    fwd_step(s, sc);
+    const SiteCode nx2 = code[s + 2];
+    fwd_step(s, cur, nx.layer);
+    cur = nx;
+    nx = nx2;
 #pragma unroll
-    for (int k = 0; k < NP; ++k) fp[k * kThreads] = make_float2(m[k], c[k]);
+    for (int k = 0; k < NP; ++k) __stcs(fp + k * kThreads, make_float2(m[k], c[k]));
     fp += kRow;
   }
 
@@ -234,7 +264,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   }
   // Backward step at site s: the het/hom site table first, then any full
   // 1000-bp chunks; split so the combine can run between fetch and finish.
-  auto bwd_fetch = [&](int s, SiteCode sc, Fetch* f) {
+  auto bwd_fetch = [&](int s, SiteCode sc, int next_layer, Fetch* f) {
     if ((s & 63) == 63 && s != pe - 1) {
 #pragma unroll
       for (int k = 0; k < NP; ++k) x[k] = word_at(gi[k], nh, s) ^ word_at(gj[k], nh, s);
@@ -245,6 +275,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
       const int het = (int)(x[k] >> 63);
       x[k] <<= 1;
       f[k] = patch_fetch(layer + het * kHetF4, m[k], c[k]);
+      prefetch_patch(bwd_tab + next_layer + (int)(x[k] >> 63) * kHetF4 + kPatchF4 * f[k].idx);
     }
   };
   auto bwd_finish = [&](SiteCode sc, const Fetch* f) {
@@ -258,13 +289,15 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     }
   };
   s = pe - 1;
-  nxt = code[s];
+  cur = code[s];
+  nx = code[s - 1];
   for (; s >= ce; --s) {
-    const SiteCode sc = nxt;
-    nxt = code[s - 1];
+    const SiteCode nx2 = code[s - 2];
     Fetch f[NP];
-    bwd_fetch(s, sc, f);
-    bwd_finish(sc, f);
+    bwd_fetch(s, cur, nx.layer, f);
+    bwd_finish(cur, f);
+    cur = nx;
+    nx = nx2;
   }
   // forward-state ring: q[i] holds the state of site s - i
   const float2* fq = slot + (int64_t)(ce - 1 - cs) * kRow + j0;
@@ -273,7 +306,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   for (int i = 0; i < kFwdPrefetch; ++i) {
 #pragma unroll
     for (int k = 0; k < NP; ++k)
-      q[i][k] = (ce - 1 - i >= cs) ? fq[k * kThreads] : make_float2(0.0f, 0.0f);
+      q[i][k] = (ce - 1 - i >= cs) ? __ldlu(fq + k * kThreads) : make_float2(0.0f, 0.0f);
     fq -= kRow;
   }
   int64_t o = t.out_off + (int64_t)(ce - 1 - t.out_row0) * t.ldo + j0;
@@ -291,10 +324,10 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     const bool ahead = s - kFwdPrefetch >= cs;
 #pragma unroll
     for (int k = 0; k < NP; ++k)
-      q[kFwdPrefetch - 1][k] = ahead ? fq[k * kThreads] : make_float2(0.0f, 0.0f);
+      q[kFwdPrefetch - 1][k] = ahead ? __ldlu(fq + k * kThreads) : make_float2(0.0f, 0.0f);
     fq -= kRow;
-    const SiteCode sc = nxt;
-    nxt = code[s - 1];
+    const SiteCode sc = cur;
+    const SiteCode nx2 = code[s - 2];
     float mb[NP], cb[NP];
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
@@ -303,19 +336,28 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     }
     Fetch fe[NP];
     const bool more = s > cs;
-    if (more) bwd_fetch(s, sc, fe);
+    if (more) bwd_fetch(s, sc, nx.layer, fe);
 #pragma unroll
     for (int k = 0; k < NP; ++k)
       if (live[k]) combine_store(t, o + k * kThreads, f[k], mb[k], cb[k], ci, post);
     o -= t.ldo;
     if (more) bwd_finish(sc, fe);
+    cur = nx;
+    nx = nx2;
   }
 }
 
 // Persistent scan: each CTA takes tasks from a global counter until none are
 // left; its forward-state slot is reused task after task.
+// Resident CTAs per SM the register budget is fitted to (128 threads each):
+// 6 leaves the single-pair kernel ~80 registers and no spills, which measured
+// faster than 8 CTAs with spills.
+#ifndef GSMC_MIN_CTAS
+#define GSMC_MIN_CTAS 6
+#endif
+
 template <int NP>
-__global__ void __launch_bounds__(kThreads, NP == 1 ? 8 : 4)
+__global__ void __launch_bounds__(kThreads, NP == 1 ? GSMC_MIN_CTAS : GSMC_MIN_CTAS / 2)
     fb_scan_persistent(const ScanArgs a) {
   // The task descriptor lives in shared memory: its fields are uniform across
   // the CTA and read only where used, so they cost no registers.

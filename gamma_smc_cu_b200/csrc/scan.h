@@ -14,6 +14,8 @@ struct SiteCode {
   int layer;
   int chunks;
 };
+// Zero entries stored before site 0 and after the last site of the code array.
+constexpr int kCodePad = 2;
 
 // Output selection of a task.
 enum TaskFlags { kTaskCI = 1, kTaskPosterior = 2 };
@@ -39,7 +41,7 @@ struct Task {
 struct ScanArgs {
   const ulonglong2* geno;   // [n_groups][n_haps]: 128 sites per entry, bit b of .x/.y = site 128g+b / 128g+64+b
   int64_t n_haps;
-  const SiteCode* code;     // [n_sites], with one zero entry before and after
+  const SiteCode* code;     // [n_sites], with kCodePad zero entries before and after
   const float4* site_tab;   // [2 directions][L][hom, het][2450][2]
   const float4* chunk_tab;  // [2450][2]
   int L;

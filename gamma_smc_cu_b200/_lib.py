@@ -55,6 +55,9 @@ SIGNATURES = {
                                       c_int, c_i32p, c_f32p, c_f32p, c_f32p, c_f32p, c_f32p]),
     "gsmc_run_fb_blockwise_device": (c_int, [c_vp, c_vp, c_vp, c_i64, c_i64, c_i64, c_int, c_vp,
                                              c_vp, c_vp, c_vp, c_vp, c_i64, c_i64, c_vp]),
+    "gsmc_run_fb_blockwise_device_noalloc": (c_int, [c_vp, c_vp, c_vp, c_i64, c_i64, c_i64, c_int,
+                                                     c_vp, c_vp, c_vp, c_vp, c_vp, c_i64, c_i64,
+                                                     c_vp]),
     "gsmc_ctx_scratch_bytes": (c_int, [c_vp, c_u64p]),
     "gsmc_ctx_timing": (c_int, [c_vp, c_int]),
     "gsmc_ctx_timing_read": (c_int, [c_vp, ctypes.POINTER(ctypes.c_double), c_i64p,

@@ -15,6 +15,7 @@
 #include <tuple>
 #include <vector>
 
+#include "ctx_view.h"
 #include "gsmc_b200.h"
 #include "hostcopy.h"
 #include "scan.h"
@@ -761,3 +762,23 @@ int gsmc_ctx_table_layer(const gsmc_ctx* ctx, int table, int layer, float* out) 
 }
 
 }  // extern "C"
+
+namespace gsmc {
+
+bool ctx_view(const gsmc_ctx* ctx, CtxView* out) {
+  if (!ctx || !out) return false;
+  out->device = ctx->device;
+  out->n_haps = ctx->n_haps;
+  out->n_sites = ctx->n_sites;
+  out->geno = ctx->geno;
+  out->code = ctx->code;
+  out->site_tab = ctx->tables->site;
+  out->chunk_tab = ctx->tables->chunk;
+  out->L = ctx->tables->L;
+  out->ne = ctx->ne;
+  return true;
+}
+
+int set_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
+}  // namespace gsmc

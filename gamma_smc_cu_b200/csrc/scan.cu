@@ -20,332 +20,11 @@
 #include <stdint.h>
 
 #include "scan.h"
+#include "scan_device.cuh"
 #include "tables.h"
 
 namespace gsmc {
 namespace {
-
-// Grid bounds and steps as the scan kernels hard-code them
-// (src/kernels/gamma_smc_flow.cu:10-17).
-constexpr float kMLo = -5.0f;
-constexpr float kMHi = 2.0f;
-constexpr float kCLo = -2.0f;
-constexpr float kCHi = 0.0f;
-constexpr float kMStep = (kMHi - kMLo) / (kRows - 1);
-constexpr float kCStep = (kCHi - kCLo) / (kCols - 1);
-constexpr float kMInv = 1.0f / kMStep;
-constexpr float kCInv = 1.0f / kCStep;
-
-// Bilinear lookup of (m, c) in one patch layer, identical to the reference's
-// clamp / truncate / keep-the-upper-cell interpolation.  Split in two so
-// independent work can be scheduled between the loads and their use.
-struct Fetch {
-  float4 a, b;  // m corners and c corners of the patch
-  float wm, wc;
-  int idx;      // patch index within the layer
-};
-
-// Hint the patch a pair will most likely read at its next site (same cell,
-// next site's layer, next site's hom/het half) into L1.
-__device__ __forceinline__ void prefetch_patch(const float4* p) {
-#ifdef GSMC_PREFETCH_NEXT
-  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
-#else
-  (void)p;
-#endif
-}
-
-__device__ __forceinline__ Fetch patch_fetch(const float4* __restrict__ layer, float m, float c) {
-  float fm = __fmul_rn(__fsub_rn(m, kMLo), kMInv);
-  float fc = __fmul_rn(__fsub_rn(c, kCLo), kCInv);
-  fm = fmaxf(0.0f, fminf(fm, (float)(kRows - 1)));
-  fc = fmaxf(0.0f, fminf(fc, (float)(kCols - 1)));
-  // Lower-left corner: the reference truncates (fm >= 0, so floor) and moves
-  // an index that lands on the last row/column down by one.  floor(min(x,
-  // last - 0.5)) is both at once, and the weight stays x - corner.
-  const float rf = floorf(fminf(fm, (float)kPatchRows - 0.5f));
-  const float qf = floorf(fminf(fc, (float)kPatchCols - 0.5f));
-  Fetch f;
-  f.wm = __fsub_rn(fm, rf);
-  f.wc = __fsub_rn(fc, qf);
-  // rf * 49 + qf is an exact integer below 2450; adding 2^23 places it in the
-  // low mantissa bits, so the patch index needs no conversion instruction.
-  const int idx = __float_as_int(__fadd_rn(__fmaf_rn(rf, (float)kPatchCols, qf), 8388608.0f)) -
-                  0x4B000000;
-  // One 256-bit read-only load of the 32-byte patch: m corners (r,q) (r,q+1)
-  // (r+1,q) (r+1,q+1), then the c corners.  Patches are 32-byte aligned:
-  // table bases come from cudaMalloc and every layer, hom/het half and patch
-  // offset is a multiple of 32 bytes.
-  f.idx = idx;
-  const float4* p = layer + kPatchF4 * idx;
-  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-      : "=f"(f.a.x), "=f"(f.a.y), "=f"(f.a.z), "=f"(f.a.w), "=f"(f.b.x), "=f"(f.b.y),
-        "=f"(f.b.z), "=f"(f.b.w)
-      : "l"(p));
-  return f;
-}
-
-__device__ __forceinline__ void patch_interp(const Fetch& f, float& m, float& c) {
-  const float vc = __fsub_rn(1.0f, f.wc), vm = __fsub_rn(1.0f, f.wm);
-  m = __fmaf_rn(f.wm, __fmaf_rn(f.wc, f.a.w, __fmul_rn(vc, f.a.z)),
-                __fmul_rn(vm, __fmaf_rn(f.wc, f.a.y, __fmul_rn(vc, f.a.x))));
-  c = __fmaf_rn(f.wm, __fmaf_rn(f.wc, f.b.w, __fmul_rn(vc, f.b.z)),
-                __fmul_rn(vm, __fmaf_rn(f.wc, f.b.y, __fmul_rn(vc, f.b.x))));
-}
-
-__device__ __forceinline__ void patch_lookup(const float4* __restrict__ layer, float& m,
-                                             float& c) {
-  const Fetch f = patch_fetch(layer, m, c);
-  patch_interp(f, m, c);
-}
-
-// 10^x by the bit construction upstream gamma_smc uses (Schraudolph 1999,
-// "A fast, compact approximation of the exponential function"): the float
-// whose bits are trunc(C2 * (x * ln10) + C1) (src/kernels/gamma_smc_flow.cu:
-// 112-121).
-__device__ __forceinline__ float pow10_bits(float x) {
-  const float kLn10 = 2.30258509299f;
-  const float kC1 = 1064872507.1541044f;
-  const float kC2 = 12102203.161561485f;
-  return __int_as_float(__float2int_rz(__fmaf_rn(kC2, __fmul_rn(x, kLn10), kC1)));
-}
-
-__device__ __forceinline__ uint64_t word_at(const ulonglong2* g, int64_t nh, int s) {
-  const ulonglong2 v = __ldg(g + (int64_t)(s >> 7) * nh);
-  return (s & 64) ? v.y : v.x;
-}
-
-// Posterior combine at one core site: forward state f, backward state (m, c)
-// (src/kernels/gamma_smc_flow.cu:708-734).
-__device__ __forceinline__ void combine_store(const Task& t, int64_t o, float2 f, float m, float c,
-                                              bool ci, bool post) {
-  const float ab = -2.0f * c;
-  const float ba = pow10_bits(ab), bb = pow10_bits(__fsub_rn(ab, m));
-  const float af = -2.0f * f.y;
-  const float fa = pow10_bits(af), fb = pow10_bits(__fsub_rn(af, f.x));
-  const float a_s = __fsub_rn(__fadd_rn(fa, ba), 1.0f);
-  const float b_s = __fsub_rn(__fadd_rn(fb, bb), 1.0f);
-  const float mg = __fmul_rn(__fdiv_rn(a_s, fmaxf(b_s, 1e-10f)), t.unscale);
-  __stcs(t.out[0] + o, mg);
-  if (ci) {
-    // Wilson-Hilferty 95% bounds (src/kernels/gamma_smc_flow.cu:724-733).
-    const float inv9a = __frcp_rn(__fmul_rn(9.0f, fmaxf(a_s, 1.0f)));
-    const float sq = __fsqrt_rn(inv9a);
-    const float base = __fsub_rn(1.0f, inv9a);
-    const float lo = fmaxf(__fmaf_rn(-1.96f, sq, base), 0.0f);
-    const float up = __fmaf_rn(1.96f, sq, base);
-    __stcs(t.out[1] + o, fmaxf(__fmul_rn(__fmul_rn(__fmul_rn(mg, lo), lo), lo), 0.0f));
-    __stcs(t.out[2] + o, __fmul_rn(__fmul_rn(__fmul_rn(mg, up), up), up));
-  }
-  if (post) {
-    __stcs(t.out[3] + o, a_s);
-    __stcs(t.out[4] + o, b_s);
-  }
-}
-
-// Forward states are read back this many sites ahead of their use so the
-// DRAM latency of that stream is hidden behind the scan's own lookups.  They
-// and the outputs are single-use streams: stored with evict-first (.cs) and
-// read with last-use (.lu) hints so they do not displace table patches.
-constexpr int kFwdPrefetch = 4;
-constexpr int kThreads = 128;
-
-// One task: this thread's NP pairs over the task's padded window.  The
-// forward states live in this CTA's slot, rows of kThreads * NP pairs.
-template <int NP>
-__device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, float2* slot) {
-  constexpr int kRow = kThreads * NP;
-  const int64_t nh = a.n_haps;
-  const int ps = t.ps, cs = t.cs, ce = t.ce, pe = t.pe;
-  const bool ci = (t.flags & kTaskCI) != 0, post = (t.flags & kTaskPosterior) != 0;
-  const int j0 = threadIdx.x;
-  if (j0 >= t.pair_count) return;
-
-  const ulonglong2* gi[NP];
-  const ulonglong2* gj[NP];
-  bool live[NP];
-#pragma unroll
-  for (int k = 0; k < NP; ++k) {
-    const int j = j0 + k * kThreads;
-    int hi = 0, hj = 0;
-    live[k] = j < t.pair_count;
-    if (live[k]) {
-      hi = a.pi[t.pair_begin + j];
-      hj = a.pj[t.pair_begin + j];
-      // Device-side pair indices are not validated by the host: a bad pair is
-      // skipped (outputs untouched) instead of reading out of bounds.
-      if (hi < 0 || hi >= nh || hj < 0 || hj >= nh) {
-        live[k] = false;
-        hi = hj = 0;
-      }
-    }
-    gi[k] = a.geno + hi;
-    gj[k] = a.geno + hj;
-  }
-  // code[-2..-1] and code[n_sites..n_sites+1] exist (zero padding), so the
-  // two-sites-ahead code prefetches below never leave the array.
-  const SiteCode* __restrict__ code = a.code;
-  const float4* __restrict__ fwd_tab = a.site_tab;
-  const float4* __restrict__ bwd_tab = a.site_tab + (size_t)a.L * kLayerF4;
-  const float4* __restrict__ chunk = a.chunk_tab;
-
-  // ---- forward: [ps, ce); states stored for [cs, ce) ----
-  float m[NP], c[NP];
-  uint64_t x[NP];
-#pragma unroll
-  for (int k = 0; k < NP; ++k) {
-    m[k] = 0.0f;
-    c[k] = 0.0f;
-    x[k] = (word_at(gi[k], nh, ps) ^ word_at(gj[k], nh, ps)) >> (ps & 63);
-  }
-  float2* fp = slot + j0;
-  // Gap codes run two sites ahead: `cur` is this site's, `nx` the next one's
-  // (already in registers, so the next-site prefetch does not wait on it).
-  auto fwd_step = [&](int s, SiteCode sc, int next_layer) {
-    if ((s & 63) == 0 && s != ps) {
-#pragma unroll
-      for (int k = 0; k < NP; ++k) x[k] = word_at(gi[k], nh, s) ^ word_at(gj[k], nh, s);
-    }
-    if (sc.chunks) {
-      for (int u = 0; u < sc.chunks; ++u) {
-#pragma unroll
-        for (int k = 0; k < NP; ++k) patch_lookup(chunk, m[k], c[k]);
-      }
-    }
-    const float4* layer = fwd_tab + sc.layer;
-    Fetch f[NP];
-#pragma unroll
-    for (int k = 0; k < NP; ++k) {
-      const int het = (int)(x[k] & 1ull);
-      x[k] >>= 1;
-      f[k] = patch_fetch(layer + het * kHetF4, m[k], c[k]);
-      prefetch_patch(fwd_tab + next_layer + (int)(x[k] & 1ull) * kHetF4 + kPatchF4 * f[k].idx);
-    }
-#pragma unroll
-    for (int k = 0; k < NP; ++k) patch_interp(f[k], m[k], c[k]);
-  };
-  int s = ps;
-  // a window that does not start at site 0 enters its first site by 1 bp
-  SiteCode cur = ps > 0 ? SiteCode{0, 0} : code[s];
-  SiteCode nx = code[s + 1];
-  {
-    const SiteCode nx2 = code[s + 2];
-    fwd_step(s, cur, nx.layer);
-    cur = nx;
-    nx = nx2;
-  }
-  if (s >= cs) {
-#pragma unroll
-    for (int k = 0; k < NP; ++k) __stcs(fp + k * kThreads, make_float2(m[k], c[k]));
-    fp += kRow;
-  }
-  for (++s; s < cs; ++s) {
-    const SiteCode nx2 = code[s + 2];
-    fwd_step(s, cur, nx.layer);
-    cur = nx;
-    nx = nx2;
-  }
-  for (; s < ce; ++s) {
-    const SiteCode nx2 = code[s + 2];
-    fwd_step(s, cur, nx.layer);
-    cur = nx;
-    nx = nx2;
-#pragma unroll
-    for (int k = 0; k < NP; ++k) __stcs(fp + k * kThreads, make_float2(m[k], c[k]));
-    fp += kRow;
-  }
-
-  // ---- backward: [pe-1 .. cs]; posterior at core sites ----
-#pragma unroll
-  for (int k = 0; k < NP; ++k) {
-    m[k] = 0.0f;
-    c[k] = 0.0f;
-    x[k] = (word_at(gi[k], nh, pe - 1) ^ word_at(gj[k], nh, pe - 1)) << (63 - ((pe - 1) & 63));
-  }
-  // Backward step at site s: the het/hom site table first, then any full
-  // 1000-bp chunks; split so the combine can run between fetch and finish.
-  auto bwd_fetch = [&](int s, SiteCode sc, int next_layer, Fetch* f) {
-    if ((s & 63) == 63 && s != pe - 1) {
-#pragma unroll
-      for (int k = 0; k < NP; ++k) x[k] = word_at(gi[k], nh, s) ^ word_at(gj[k], nh, s);
-    }
-    const float4* layer = bwd_tab + sc.layer;
-#pragma unroll
-    for (int k = 0; k < NP; ++k) {
-      const int het = (int)(x[k] >> 63);
-      x[k] <<= 1;
-      f[k] = patch_fetch(layer + het * kHetF4, m[k], c[k]);
-      prefetch_patch(bwd_tab + next_layer + (int)(x[k] >> 63) * kHetF4 + kPatchF4 * f[k].idx);
-    }
-  };
-  auto bwd_finish = [&](SiteCode sc, const Fetch* f) {
-#pragma unroll
-    for (int k = 0; k < NP; ++k) patch_interp(f[k], m[k], c[k]);
-    if (sc.chunks) {
-      for (int u = 0; u < sc.chunks; ++u) {
-#pragma unroll
-        for (int k = 0; k < NP; ++k) patch_lookup(chunk, m[k], c[k]);
-      }
-    }
-  };
-  s = pe - 1;
-  cur = code[s];
-  nx = code[s - 1];
-  for (; s >= ce; --s) {
-    const SiteCode nx2 = code[s - 2];
-    Fetch f[NP];
-    bwd_fetch(s, cur, nx.layer, f);
-    bwd_finish(cur, f);
-    cur = nx;
-    nx = nx2;
-  }
-  // forward-state ring: q[i] holds the state of site s - i
-  const float2* fq = slot + (int64_t)(ce - 1 - cs) * kRow + j0;
-  float2 q[kFwdPrefetch][NP];
-#pragma unroll
-  for (int i = 0; i < kFwdPrefetch; ++i) {
-#pragma unroll
-    for (int k = 0; k < NP; ++k)
-      q[i][k] = (ce - 1 - i >= cs) ? __ldlu(fq + k * kThreads) : make_float2(0.0f, 0.0f);
-    fq -= kRow;
-  }
-  int64_t o = t.out_off + (int64_t)(ce - 1 - t.out_row0) * t.ldo + j0;
-  // unrolled by the ring depth so the ring rotation is register renaming
-#pragma unroll kFwdPrefetch
-  for (s = ce - 1; s >= cs; --s) {
-    float2 f[NP];
-#pragma unroll
-    for (int k = 0; k < NP; ++k) f[k] = q[0][k];
-#pragma unroll
-    for (int i = 0; i + 1 < kFwdPrefetch; ++i) {
-#pragma unroll
-      for (int k = 0; k < NP; ++k) q[i][k] = q[i + 1][k];
-    }
-    const bool ahead = s - kFwdPrefetch >= cs;
-#pragma unroll
-    for (int k = 0; k < NP; ++k)
-      q[kFwdPrefetch - 1][k] = ahead ? __ldlu(fq + k * kThreads) : make_float2(0.0f, 0.0f);
-    fq -= kRow;
-    const SiteCode sc = cur;
-    const SiteCode nx2 = code[s - 2];
-    float mb[NP], cb[NP];
-#pragma unroll
-    for (int k = 0; k < NP; ++k) {
-      mb[k] = m[k];
-      cb[k] = c[k];
-    }
-    Fetch fe[NP];
-    const bool more = s > cs;
-    if (more) bwd_fetch(s, sc, nx.layer, fe);
-#pragma unroll
-    for (int k = 0; k < NP; ++k)
-      if (live[k]) combine_store(t, o + k * kThreads, f[k], mb[k], cb[k], ci, post);
-    o -= t.ldo;
-    if (more) bwd_finish(sc, fe);
-    cur = nx;
-    nx = nx2;
-  }
-}
 
 // Persistent scan: each CTA takes tasks from a global counter until none are
 // left; its forward-state slot is reused task after task.

@@ -130,6 +130,25 @@ int gsmc_run_fb_blockwise_device(gsmc_ctx* ctx, const int32_t* d_pair_i,
                                  float* d_upper, float* d_alpha, float* d_beta,
                                  int64_t ld_out, int64_t out_col0, void* stream);
 
+/*
+ * Same as gsmc_run_fb_blockwise_device, but the call allocates no device
+ * memory: for callers that cannot allocate during the call (inside CUDA graph
+ * stream capture, under a framework allocator that owns the device memory,
+ * or in latency-bound loops that cannot pay for cudaMalloc's device sync).
+ * Its scratch is a fixed 128 MiB device array held by every GPU that loads
+ * the library until exit; core_block_sites above 131,071 (one CTA slot no
+ * longer fits) is rejected with GSMC_E_INVALID.  All calls share that array:
+ * calls that overlap on the GPU race and must be serialised by the caller.
+ * The first call on each device looks the array's address up; make it before
+ * any stream capture.  No counterpart in the reference.
+ */
+int gsmc_run_fb_blockwise_device_noalloc(gsmc_ctx* ctx, const int32_t* d_pair_i,
+                                         const int32_t* d_pair_j, int64_t n_pairs,
+                                         int64_t core_block_sites, int64_t flank_sites,
+                                         int flags, float* d_mean, float* d_lower,
+                                         float* d_upper, float* d_alpha, float* d_beta,
+                                         int64_t ld_out, int64_t out_col0, void* stream);
+
 /* Bytes of device scratch the context currently holds (forward-state pool). */
 int gsmc_ctx_scratch_bytes(const gsmc_ctx* ctx, uint64_t* bytes);
 

@@ -46,6 +46,10 @@ METRIC = "pair-site posteriors/sec"
 UNIT = "pair-sites/s"
 BYTES_MEAN_ONLY = 4.25      # 4 B fp32 mean + 2 genotype bits per pair-site
 BYTES_FULL_POSTERIOR = 12.25
+# DRAM bytes (read + write) the scan kernel moves per core pair-site in
+# mean-only mode, from an ncu capture of the chromprof case (profiles/
+# fb_scan_persistent_chromprof.md): 16 B forward-state round trip + 4 B output.
+TRAFFIC_PER_PAIR_SITE = 20.0
 
 
 def parse():
@@ -58,6 +62,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-full-posterior", action="store_true")
     return ap.parse_args()
 
 
@@ -151,19 +156,18 @@ def cpu_baseline_sample(G, pos, pairs, core, flank, mu, rho, target_s=12.0):
     threads = os.cpu_count() or 1
     O.tables_for(DEFAULT_FLOW_FIELD, 1e4, mu, rho)
     S = G.shape[1]
-    probe = pairs[:max(8, threads)]
-    t0 = time.perf_counter()
-    O.run_fb_blockwise(G, pos, [tuple(p) for p in probe], 1e4, mu, rho, DEFAULT_FLOW_FIELD,
-                       core, flank, True, False, threads)
-    dt = time.perf_counter() - t0
-    n_sample = int(min(len(pairs), max(len(probe), len(probe) * target_s / max(dt, 1e-3))))
-    sample = pairs[:n_sample]
-    t0 = time.perf_counter()
-    O.run_fb_blockwise(G, pos, [tuple(p) for p in sample], 1e4, mu, rho, DEFAULT_FLOW_FIELD,
-                       core, flank, True, False, threads)
-    dt = time.perf_counter() - t0
-    return {"value": n_sample * S / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{n_sample} pairs x {S} sites, blockwise core={core} flank={flank}, "
+    # grow the pair sample until one run takes a few seconds, at most ~target_s
+    n = min(len(pairs), max(4 * threads, 64))
+    while True:
+        t0 = time.perf_counter()
+        O.run_fb_blockwise(G, pos, [tuple(p) for p in pairs[:n]], 1e4, mu, rho,
+                           DEFAULT_FLOW_FIELD, core, flank, True, False, threads)
+        dt = time.perf_counter() - t0
+        if dt >= target_s / 3 or n >= len(pairs):
+            break
+        n = min(len(pairs), int(n * min(8.0, max(2.0, target_s / max(dt, 1e-3)))))
+    return {"value": n * S / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} pairs x {S} sites, blockwise core={core} flank={flank}, "
                       f"mean_only, {dt:.1f} s"}
 
 
@@ -254,7 +258,6 @@ def main():
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    ms = ctypes_double()
     _lib.check(L.gsmc_ctx_timing_read(ctx.handle, None, None, None))
     _lib.check(L.gsmc_ctx_timing(ctx.handle, 1))
     if world > 1:
@@ -289,7 +292,14 @@ def main():
     sample = out[::max(1, S // 64), ::max(1, P // 64)]
     assert bool(torch.isfinite(sample).all()) and bool((sample > 0).all()), "bad posterior"
     del out
+    ctx.close()
     torch.cuda.empty_cache()
+    traffic = (TRAFFIC_PER_PAIR_SITE * psites.value / launches.value
+               if launches.value and args.workload != "small" else None)
+
+    full = None
+    if args.workload == "chrom" and not args.no_full_posterior:
+        full = run_full_posterior(G, pos, pairs, args.steps, args.warmup, dev)
 
     e2e = None
     if not args.no_e2e:
@@ -308,10 +318,11 @@ def main():
                        "parallelism": f"pairs replicated per rank x{world} (weak)"},
             "gpu_launches": int(launches.value),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None,
-                         "peak_kind": peak_kind, "kernel": "fb_scan_kernel<false,false>",
+                         "frac": achieved / hbm, "traffic": traffic,
+                         "peak_kind": peak_kind, "kernel": "fb_scan_persistent<1>",
                          "kernel_ms_per_step": kms.value / args.steps,
                          "bytes_per_pair_site": BYTES_MEAN_ONLY},
+            "full_posterior": full,
             "clocks": clk.summary(),
             "e2e": e2e,
             "cpu_baseline": cpu,
@@ -321,9 +332,78 @@ def main():
         dist.destroy_process_group()
 
 
-def ctypes_double():
+def timed_device_run(ctx, d_pi, d_pj, P, S, core, flank, flags, outs, steps, warmup, dev):
+    """Event-timed device-resident blockwise runs; returns (ms per step,
+    kernel ms per step, launches, pair-sites)."""
     import ctypes
-    return ctypes.c_double()
+    import torch
+    from gamma_smc_cu_b200 import _lib
+    L = _lib.load()
+    stream = torch.cuda.current_stream(dev)
+    ptrs = [o.data_ptr() if o is not None else None for o in outs]
+
+    def step():
+        _lib.check(L.gsmc_run_fb_blockwise_device(
+            ctx.handle, d_pi.data_ptr(), d_pj.data_ptr(), P, core, flank, flags, *ptrs, P, 0,
+            stream.cuda_stream))
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    _lib.check(L.gsmc_ctx_timing_read(ctx.handle, None, None, None))
+    _lib.check(L.gsmc_ctx_timing(ctx.handle, 1))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    kms = ctypes.c_double()
+    launches = ctypes.c_int64()
+    psites = ctypes.c_double()
+    _lib.check(L.gsmc_ctx_timing_read(ctx.handle, ctypes.byref(kms), ctypes.byref(launches),
+                                      ctypes.byref(psites)))
+    _lib.check(L.gsmc_ctx_timing(ctx.handle, 0))
+    return e0.elapsed_time(e1) / steps, kms.value / steps, launches.value, psites.value
+
+
+def run_full_posterior(G, pos, pairs, steps, warmup, dev, n_sites=50_000):
+    """North-star roofline case: mean + posterior alpha/beta (12.25 B per
+    pair-site) on the first 50,000 sites of the chromosome cohort, all pairs,
+    blockwise with the API's auto core and flank 2048, outputs in HBM."""
+    import torch
+    from gamma_smc_cu_b200 import _core, _lib
+    from gamma_smc_cu_b200.infer import _estimate_scaled_params, _recommend_core_block_size
+    Gs = np.ascontiguousarray(G[:, :n_sites])
+    ps = np.ascontiguousarray(pos[:n_sites])
+    S, P = Gs.shape[1], len(pairs)
+    mu, rho = _estimate_scaled_params(Gs, ps, 1.25e-8, 1e-8, 1e4)
+    ctx = _core.FlowContext(Gs, ps, 1e4, mu, rho, _core.DEFAULT_FLOW_FIELD, 0)
+    free, _ = _core.cuda_mem_info()
+    core, _ = _recommend_core_block_size(S, P, True, 2048, free)
+    d_pi = torch.from_numpy(np.ascontiguousarray(pairs[:, 0])).to(dev)
+    d_pj = torch.from_numpy(np.ascontiguousarray(pairs[:, 1])).to(dev)
+    outs = [torch.empty((S, P), dtype=torch.float32, device=dev) for _ in range(3)]
+    ms, kms, launches, psites = timed_device_run(
+        ctx, d_pi, d_pj, P, S, core, 2048, _lib.GSMC_POSTERIOR,
+        [outs[0], None, None, outs[1], outs[2]], steps, warmup, dev)
+    hbm, kind = peaks()
+    steps_ = max(1, steps)
+    achieved = psites / steps_ * BYTES_FULL_POSTERIOR / (kms / 1e3) / 1e9
+    recon = (outs[1][::997, ::61] / outs[2][::997, ::61]) * 2e4
+    ok = bool(torch.allclose(recon, outs[0][::997, ::61], rtol=1e-4, atol=1e-2))
+    del outs
+    ctx.close()
+    torch.cuda.empty_cache()
+    return {"workload": f"chrom 50k-site slice: 356 haps x {S} sites x {P} pairs, mean+alpha+beta",
+            "core_block_sites": int(core), "flank_sites": 2048,
+            "value": P * S / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
+            "gpu_launches": int(launches), "posterior_consistent": ok,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "peak_kind": kind,
+                         "bytes_per_pair_site": BYTES_FULL_POSTERIOR, "traffic": None,
+                         "kernel_ms_per_step": kms}}
 
 
 def run_e2e(G, pos, pairs, core, flank, steps):

@@ -63,6 +63,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-full-posterior", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--plain-jobs", type=int, default=48,
+                    help="jobs of the mix timed through the plain per-call path")
     return ap.parse_args()
 
 
@@ -292,6 +296,10 @@ def main():
     sample = out[::max(1, S // 64), ::max(1, P // 64)]
     assert bool(torch.isfinite(sample).all()) and bool((sample > 0).all()), "bad posterior"
     del out
+    torch.cuda.empty_cache()
+    batched = None
+    if args.workload == "chrom" and not args.no_batched:
+        batched = run_batched(ctx, G, dev, args.plain_jobs)
     ctx.close()
     torch.cuda.empty_cache()
     traffic = (TRAFFIC_PER_PAIR_SITE * psites.value / launches.value
@@ -300,6 +308,10 @@ def main():
     full = None
     if args.workload == "chrom" and not args.no_full_posterior:
         full = run_full_posterior(G, pos, pairs, args.steps, args.warmup, dev)
+
+    served = None
+    if args.workload == "chrom" and not args.no_served:
+        served = run_served(dev)
 
     e2e = None
     if not args.no_e2e:
@@ -323,6 +335,8 @@ def main():
                          "kernel_ms_per_step": kms.value / args.steps,
                          "bytes_per_pair_site": BYTES_MEAN_ONLY},
             "full_posterior": full,
+            "batched": batched,
+            "served": served,
             "clocks": clk.summary(),
             "e2e": e2e,
             "cpu_baseline": cpu,
@@ -404,6 +418,165 @@ def run_full_posterior(G, pos, pairs, steps, warmup, dev, n_sites=50_000):
                          "frac": achieved / hbm, "peak_kind": kind,
                          "bytes_per_pair_site": BYTES_FULL_POSTERIOR, "traffic": None,
                          "kernel_ms_per_step": kms}}
+
+
+def _max_rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-30))) if a.size else 0.0
+
+
+def run_batched(ctx, G, dev, plain_jobs):
+    """Uneven batch: 512 jobs (seed 5) over the chromosome cohort -- pair
+    count log-uniform in [1, 4096], window log-uniform in [1e3, 2e5] sites --
+    in one persistent launch with the autotuned launch shape and
+    sites-per-chunk, against the plain per-call path (one
+    FlowContext.run_fb_window call per job, host outputs)."""
+    import torch
+    from gamma_smc_cu_b200 import synthetic
+    from gamma_smc_cu_b200.batch import DeviceBatch, Executor, Job, Layout, _count_tasks
+    from gamma_smc_cu_b200.tune import autotune, executor_kwargs
+    jobs = [Job(**j) for j in synthetic.job_mix(G.shape[0], G.shape[1], 512, seed=5)]
+    total = float(sum(j.pair_sites for j in jobs))
+    t0 = time.perf_counter()
+    tuned = autotune(ctx, jobs, use_cache=False)
+    tune_s = time.perf_counter() - t0
+    kw = executor_kwargs(tuned)
+    ex = Executor(ctx, max_tasks=_count_tasks(jobs, kw) + 16, use_graph=True, **kw)
+    st = torch.cuda.Stream(dev)
+    # device-resident: pairs uploaded, outputs stay in HBM
+    b = DeviceBatch(Layout(jobs), dev)
+    b.allocate(st)
+    with torch.cuda.stream(st):
+        b.d_pairs.copy_(b.h_pairs, non_blocking=True)
+    run = lambda: ex.run(b.layout, b.d_pairs.data_ptr(), b.d_out.data_ptr(), st.cuda_stream)
+    for _ in range(2):
+        run()
+    st.synchronize()
+    ex.timing(True)
+    ex.timing_read()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = 3
+    e0.record(st)
+    for _ in range(reps):
+        run()
+    e1.record(st)
+    e1.synchronize()
+    dev_ms = e0.elapsed_time(e1) / reps
+    kms, launches, _ = ex.timing_read()
+    ex.timing(False)
+    del b
+    torch.cuda.empty_cache()
+    # end to end on the sample the plain path is timed on: host pairs in,
+    # host numpy results out, one launch for all jobs vs one call per job
+    sample = jobs[:plain_jobs]
+    sample_ps = float(sum(j.pair_sites for j in sample))
+    t0 = time.perf_counter()
+    bs = DeviceBatch(Layout(sample), dev)
+    bs.launch(ex, st)
+    got = [{k: np.array(v) for k, v in r.items()} for r in bs.results()]
+    batched_s = time.perf_counter() - t0
+    del bs
+    torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    want = [ctx.run_fb_window(j.pairs, j.site_begin, j.site_end) for j in sample]
+    plain_s = time.perf_counter() - t0
+    err = max(_max_rel(g["mean"], w["mean"]) for g, w in zip(got, want))
+    ex.close()
+    return {"workload": "512 jobs (seed 5) over the chromosome cohort: pairs log-uniform "
+                        "[1, 4096], windows log-uniform [1e3, 2e5] sites, mean_only",
+            "pair_sites": total, "device_ms": dev_ms, "kernel_ms": kms / max(1, reps),
+            "value": total / (dev_ms / 1e3), "unit": UNIT, "gpu_launches_per_batch": 1,
+            "tuned": {k: tuned[k] for k in ("tile_width", "pairs_per_thread",
+                                            "core_block_sites", "flank_sites")},
+            "tune_seconds": tune_s, "tune_trials": tuned["searched"],
+            "sample_jobs": len(sample), "sample_pair_sites": sample_ps,
+            "sample_batched_e2e": sample_ps / batched_s,
+            "sample_plain_per_call": sample_ps / plain_s,
+            "speedup_vs_plain": plain_s / batched_s,
+            "max_rel_mean_vs_plain": err}
+
+
+def _plain_latency(ctx, reqs, pos):
+    """Serve ``reqs`` one call at a time in arrival order (FIFO, real time);
+    returns (latencies s, pair-sites, wall s)."""
+    t0 = time.perf_counter()
+    lat = []
+    ps = 0.0
+    for r in reqs:
+        now = time.perf_counter() - t0
+        if r["t"] > now:
+            time.sleep(r["t"] - now)
+        s0 = int(np.searchsorted(pos, r["region_bp"][0]))
+        s1 = max(s0, int(np.searchsorted(pos, r["region_bp"][1])))
+        ctx.run_fb_window(r["pairs"], s0, s1, mean_only=r["mean_only"],
+                          return_posterior=r["return_posterior"])
+        lat.append(time.perf_counter() - t0 - r["t"])
+        ps += len(r["pairs"]) * (s1 - s0)
+    return np.array(lat), ps, time.perf_counter() - t0
+
+
+def _served_latency(srv, reqs):
+    t0 = time.perf_counter()
+    futs = []
+    for r in reqs:
+        now = time.perf_counter() - t0
+        if r["t"] > now:
+            time.sleep(r["t"] - now)
+        futs.append(srv.submit(r["pairs"], region_bp=r["region_bp"], mean_only=r["mean_only"],
+                               return_posterior=r["return_posterior"]))
+    for f in futs:
+        f.result()
+    st = srv.stats(reset=True)
+    return st
+
+
+def run_served(dev, rates=(10, 100, 1000, 2000), seconds=2.0, burst=300):
+    """Serving stream over the resident small cohort (40 haplotypes, 2,127
+    sites over 1 Mb): Poisson arrivals (seed 6), pair subsets log-uniform in
+    [1, 8192] (clamped to the 780 pairs), regions log-uniform in [1 kb, 5 Mb]
+    (clamped to the 1 Mb sequence), 20% full posterior.  Reports p50/p99
+    latency per rate for the served loop and for the plain per-call path
+    (FIFO, one call per query), and aggregate throughput of a burst of
+    queries submitted at once."""
+    from gamma_smc_cu_b200 import _core, synthetic
+    from gamma_smc_cu_b200.infer import _estimate_scaled_params
+    from gamma_smc_cu_b200.serve import TmrcaServer
+    G, pos = synthetic.cohort("small")
+    mu, rho = _estimate_scaled_params(G, pos, 1.25e-8, 1e-8, 1e4)
+    ctx = _core.FlowContext(G, pos, 1e4, mu, rho, _core.DEFAULT_FLOW_FIELD, 0)
+    out = {"workload": "small cohort 40 haps x 2,127 sites (1 Mb); queries: pairs log-uniform "
+                       "[1, 8192] clamped to 780, regions log-uniform [1 kb, 5 Mb] clamped to "
+                       "1 Mb, 20% full posterior", "rates": {}}
+    with TmrcaServer(ctx, positions=pos, max_inflight=3) as srv:
+        warm = synthetic.request_stream(pos, G.shape[0], 50, 0, seed=60)
+        _served_latency(srv, warm)
+        for r in warm[:10]:
+            s0 = int(np.searchsorted(pos, r["region_bp"][0]))
+            ctx.run_fb_window(r["pairs"], s0, s0 + 1)
+        # aggregate throughput: every query submitted at once
+        reqs = synthetic.request_stream(pos, G.shape[0], burst, 0, seed=6)
+        st = _served_latency(srv, reqs)
+        lat, ps, wall = _plain_latency(ctx, reqs, pos)
+        out["burst"] = {"queries": burst, "served_pair_sites_per_s": st["pair_sites_per_s"],
+                        "plain_pair_sites_per_s": ps / wall,
+                        "speedup": st["pair_sites_per_s"] / (ps / wall),
+                        "served_batches": st.get("batches")}
+        for rate in rates:
+            n = int(max(20, min(1000, rate * seconds)))
+            reqs = synthetic.request_stream(pos, G.shape[0], n, rate, seed=6)
+            st = _served_latency(srv, reqs)
+            lat, ps, wall = _plain_latency(ctx, reqs, pos)
+            out["rates"][str(rate)] = {
+                "queries": n, "served_p50_ms": st["p50_ms"], "served_p99_ms": st["p99_ms"],
+                "served_pair_sites_per_s": st["pair_sites_per_s"],
+                "served_batches": st.get("batches"),
+                "plain_p50_ms": float(np.percentile(lat, 50) * 1e3),
+                "plain_p99_ms": float(np.percentile(lat, 99) * 1e3),
+                "plain_pair_sites_per_s": ps / wall}
+    ctx.close()
+    return out
 
 
 def run_e2e(G, pos, pairs, core, flank, steps):

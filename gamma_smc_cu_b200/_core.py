@@ -163,6 +163,28 @@ class FlowContext:
                                       flags, *self._out_ptrs(out)))
         return out
 
+    def run_fb_window(self, pairs, site_begin, site_end, mean_only=True,
+                      return_posterior=False):
+        """Forward-backward over sites [site_begin, site_end) only, decoded as
+        one padded window of the reference's block kernels (a window that does
+        not start at site 0 enters its first site by 1 bp); dict of
+        [site_end - site_begin, n_pairs] float32.  One call per query."""
+        pi, pj = _split_pairs(pairs)
+        P = len(pi)
+        rows = int(site_end) - int(site_begin)
+        if rows < 0 or site_begin < 0 or site_end > self._S:
+            raise ValueError(f"site window [{site_begin}, {site_end}) is out of range for "
+                             f"{self._S} sites")
+        ci = not mean_only
+        out = self._outputs(rows, P, ci, return_posterior)
+        if P == 0 or rows == 0:
+            return out
+        flags = (GSMC_CI if ci else 0) | (GSMC_POSTERIOR if return_posterior else 0)
+        check(_lib.load().gsmc_run_fb_window(self._h, ptr(pi, _lib.c_i32p), ptr(pj, _lib.c_i32p),
+                                             P, int(site_begin), int(site_end), flags,
+                                             *self._out_ptrs(out)))
+        return out
+
     def run_fb_blockwise(self, pairs, core_block_sites=8192, flank_sites=2048,
                          pair_batch_size=256, max_streams=1, mean_only=True,
                          return_posterior=False):

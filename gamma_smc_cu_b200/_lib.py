@@ -36,6 +36,37 @@ c_vp = ctypes.c_void_p
 c_int = ctypes.c_int
 c_intp = ctypes.POINTER(ctypes.c_int)
 
+class ExecConfig(ctypes.Structure):
+    """gsmc_exec_config of include/gsmc_b200.h."""
+    _fields_ = [
+        ("tile_width", ctypes.c_int32),
+        ("pairs_per_thread", ctypes.c_int32),
+        ("core_block_sites", ctypes.c_int64),
+        ("flank_sites", ctypes.c_int64),
+        ("max_window_sites", ctypes.c_int64),
+        ("max_tasks", ctypes.c_int64),
+        ("max_pool_bytes", ctypes.c_uint64),
+        ("max_ctas", ctypes.c_int32),
+        ("use_graph", ctypes.c_int32),
+    ]
+
+
+class Job(ctypes.Structure):
+    """gsmc_job of include/gsmc_b200.h (device pointers as integers)."""
+    _fields_ = [
+        ("pair_i", ctypes.c_void_p),
+        ("pair_j", ctypes.c_void_p),
+        ("n_pairs", ctypes.c_int64),
+        ("site_begin", ctypes.c_int64),
+        ("site_end", ctypes.c_int64),
+        ("flags", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("out", ctypes.c_void_p * 5),
+        ("ld_out", ctypes.c_int64),
+        ("out_col0", ctypes.c_int64),
+    ]
+
+
 # name -> (restype, argtypes); mirrors include/gsmc_b200.h
 SIGNATURES = {
     "gsmc_last_error": (ctypes.c_char_p, []),
@@ -58,6 +89,15 @@ SIGNATURES = {
     "gsmc_run_fb_blockwise_device_noalloc": (c_int, [c_vp, c_vp, c_vp, c_i64, c_i64, c_i64, c_int,
                                                      c_vp, c_vp, c_vp, c_vp, c_vp, c_i64, c_i64,
                                                      c_vp]),
+    "gsmc_run_fb_window": (c_int, [c_vp, c_i32p, c_i32p, c_i64, c_i64, c_i64, c_int, c_f32p,
+                                   c_f32p, c_f32p, c_f32p, c_f32p]),
+    "gsmc_exec_create": (c_int, [c_vp, ctypes.POINTER(ExecConfig), ctypes.POINTER(c_vp)]),
+    "gsmc_exec_destroy": (c_int, [c_vp]),
+    "gsmc_exec_info": (c_int, [c_vp, c_intp, c_u64p, c_i64p, c_i64p]),
+    "gsmc_exec_run": (c_int, [c_vp, ctypes.POINTER(Job), c_i64, c_vp]),
+    "gsmc_exec_timing": (c_int, [c_vp, c_int]),
+    "gsmc_exec_timing_read": (c_int, [c_vp, ctypes.POINTER(ctypes.c_double), c_i64p,
+                                      ctypes.POINTER(ctypes.c_double)]),
     "gsmc_ctx_scratch_bytes": (c_int, [c_vp, c_u64p]),
     "gsmc_ctx_timing": (c_int, [c_vp, c_int]),
     "gsmc_ctx_timing_read": (c_int, [c_vp, ctypes.POINTER(ctypes.c_double), c_i64p,

@@ -20,7 +20,7 @@ LIBDIR = os.path.join(HERE, "lib")
 OBJDIR = os.path.join(HERE, "_build")
 LIB = os.path.join(LIBDIR, "libgsmc_b200.so")
 
-CUDA_SOURCES = ["scan.cu", "capi.cu", "hostcopy.cu", "noalloc.cu"]
+CUDA_SOURCES = ["scan.cu", "capi.cu", "hostcopy.cu", "exec.cu", "noalloc.cu"]
 CXX_SOURCES = ["tables.cpp"]
 HEADERS = ["scan.h", "scan_device.cuh", "tables.h", "hostcopy.h", "ctx_view.h"]
 

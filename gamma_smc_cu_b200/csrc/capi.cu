@@ -147,7 +147,7 @@ struct gsmc_ctx {
   ulonglong2* geno = nullptr;
   SiteCode* code = nullptr;  // site 0 of the code array (kCodePad entries before it)
   TableSet* tables = nullptr;
-  int pairs_per_thread = 1;  // independent chains per thread in the scan kernel
+  ScanShape shape{128, 1};  // scan launch shape of the context's own calls
   cudaStream_t stream = nullptr;
   // scratch, grown on demand and kept for the context's lifetime
   void* pool = nullptr;  // forward-state slots of the persistent CTAs
@@ -156,9 +156,8 @@ struct gsmc_ctx {
   int64_t pairs_cap = 0;
   float* stage = nullptr;  // host-path output stage: two halves
   size_t stage_bytes = 0;
-  Task* tasks[2] = {nullptr, nullptr};  // task lists of alternating launches
-  int64_t tasks_cap[2] = {0, 0};
-  int* counters = nullptr;  // work counter of each task list
+  unsigned char* tasks[2] = {nullptr, nullptr};  // task lists of alternating launches
+  size_t tasks_cap[2] = {0, 0};                  // bytes
   cudaEvent_t stage_free[2] = {nullptr, nullptr};
   cudaEvent_t launch_done[2] = {nullptr, nullptr};
   // measurement: events around scan launches while timing is on
@@ -176,7 +175,12 @@ int ensure_buffer(T** buf, size_t* cap_bytes, size_t bytes) {
   if (*buf) cudaFree(*buf);
   *buf = nullptr;
   *cap_bytes = 0;
-  CUDA_TRY(cudaMalloc(buf, bytes));
+  const cudaError_t e = cudaMalloc(buf, bytes);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    return fail(GSMC_E_NOMEM, "CUDA error: out of memory allocating %zu bytes of scratch", bytes);
+  }
+  if (e != cudaSuccess) return fail(GSMC_E_CUDA, "CUDA error: %s (scratch allocation)", cudaGetErrorString(e));
   *cap_bytes = bytes;
   return GSMC_OK;
 }
@@ -218,11 +222,30 @@ size_t free_device_bytes() {
 int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
 // Resident CTAs of the persistent kernel, optionally capped for experiments.
-int resident_ctas(const gsmc_ctx* ctx) {
-  int r = std::max(1, scan_resident_ctas(ctx->pairs_per_thread));
+int resident_ctas(ScanShape shape) {
+  int r = std::max(1, scan_resident_ctas(shape));
   if (const char* env = std::getenv("GSMC_MAX_CTAS")) r = std::max(1, std::min(r, std::atoi(env)));
   return r;
 }
+
+// Pair-steps of a task per pair: forward over [ps, ce), backward over [cs, pe).
+int64_t task_steps(const Task& t) { return (int64_t)(t.ce - t.ps) + (t.pe - t.cs); }
+
+// Longest tasks first, so the persistent grid's tail is made of short tasks.
+void order_longest_first(std::vector<Task>* tasks) {
+  std::stable_sort(tasks->begin(), tasks->end(),
+                   [](const Task& a, const Task& b) { return task_steps(a) > task_steps(b); });
+}
+
+// Host image of a device task list: head (next = 0, count) then the tasks.
+void write_task_list(const std::vector<Task>& tasks, unsigned char* dst) {
+  TaskListHead head{0, (int)tasks.size()};
+  std::memset(dst, 0, kTaskListHead);
+  std::memcpy(dst, &head, sizeof(head));
+  if (!tasks.empty()) std::memcpy(dst + kTaskListHead, tasks.data(), tasks.size() * sizeof(Task));
+}
+
+size_t task_list_bytes(size_t n) { return kTaskListHead + n * sizeof(Task); }
 
 // Where the outputs of one window go: element (s, pair j) at
 // out[k][off + (s - row0) * ldo + j].
@@ -233,10 +256,11 @@ struct WindowOut {
   int64_t row0;
 };
 
-// Append the tasks of one window for pairs [pair0, pair0 + n), pair tile by
-// pair tile; `col` is the output column of pair pair0.
-void add_window_tasks(const Block& b, int64_t pair0, int64_t n, int tile, const WindowOut& wo,
-                      int64_t col, int flags, float unscale, std::vector<Task>* tasks) {
+// Append the tasks of one window for the n pairs (pi[p], pj[p]), pair tile by
+// pair tile; `col` is the output column of pair 0.
+void add_window_tasks(const Block& b, const int32_t* pi, const int32_t* pj, int64_t n, int tile,
+                      const WindowOut& wo, int64_t col, int flags, float unscale,
+                      std::vector<Task>* tasks) {
   for (int64_t j = 0; j < n; j += tile) {
     Task t;
     std::memset(&t, 0, sizeof(t));
@@ -244,7 +268,8 @@ void add_window_tasks(const Block& b, int64_t pair0, int64_t n, int tile, const 
     t.cs = (int32_t)b.cs;
     t.ce = (int32_t)b.ce;
     t.pe = (int32_t)b.pe;
-    t.pair_begin = (int32_t)(pair0 + j);
+    t.pi = pi + j;
+    t.pj = pj + j;
     t.pair_count = (int32_t)std::min<int64_t>(tile, n - j);
     t.out_row0 = (int32_t)wo.row0;
     t.flags = flags;
@@ -256,41 +281,46 @@ void add_window_tasks(const Block& b, int64_t pair0, int64_t n, int tile, const 
   }
 }
 
+// Fill the ScanArgs fields that come from the context.
+void ctx_scan_args(const gsmc_ctx* ctx, ScanArgs* a) {
+  std::memset(a, 0, sizeof(*a));
+  a->geno = ctx->geno;
+  a->n_haps = ctx->n_haps;
+  a->code = ctx->code;
+  a->site_tab = ctx->tables->site;
+  a->chunk_tab = ctx->tables->chunk;
+  a->L = ctx->tables->L;
+}
+
 // Upload a task list into buffer `which` and launch the persistent scan with
 // up to `grid` CTAs over it; forward-state slots of slot_rows sites.
-int launch_tasks(gsmc_ctx* ctx, const std::vector<Task>& tasks, int which, const int32_t* d_pi,
-                 const int32_t* d_pj, int64_t slot_rows, int grid, cudaStream_t stream) {
+int launch_tasks(gsmc_ctx* ctx, std::vector<Task>& tasks, int which, int64_t slot_rows, int grid,
+                 cudaStream_t stream) {
   if (tasks.empty()) return GSMC_OK;
-  size_t cap = (size_t)ctx->tasks_cap[which] * sizeof(Task);
-  int rc = ensure_buffer(&ctx->tasks[which], &cap, tasks.size() * sizeof(Task));
+  order_longest_first(&tasks);
+  const size_t bytes = task_list_bytes(tasks.size());
+  int rc = ensure_buffer(&ctx->tasks[which], &ctx->tasks_cap[which], bytes);
   if (rc) return rc;
-  ctx->tasks_cap[which] = (int64_t)(cap / sizeof(Task));
-  CUDA_TRY(cudaMemcpyAsync(ctx->tasks[which], tasks.data(), tasks.size() * sizeof(Task),
-                           cudaMemcpyHostToDevice, stream));
-  CUDA_TRY(cudaMemsetAsync(ctx->counters + which, 0, sizeof(int), stream));
+  std::vector<unsigned char> image(bytes);
+  write_task_list(tasks, image.data());
+  CUDA_TRY(cudaMemcpyAsync(ctx->tasks[which], image.data(), bytes, cudaMemcpyHostToDevice, stream));
   ScanArgs a;
-  std::memset(&a, 0, sizeof(a));
-  a.geno = ctx->geno;
-  a.n_haps = ctx->n_haps;
-  a.code = ctx->code;
-  a.site_tab = ctx->tables->site;
-  a.chunk_tab = ctx->tables->chunk;
-  a.L = ctx->tables->L;
-  a.pi = d_pi;
-  a.pj = d_pj;
-  a.tasks = ctx->tasks[which];
-  a.n_tasks = (int)tasks.size();
-  a.next_task = ctx->counters + which;
+  ctx_scan_args(ctx, &a);
+  TaskListHead* head = reinterpret_cast<TaskListHead*>(ctx->tasks[which]);
+  a.next = &head->next;
+  a.count = &head->count;
+  a.tasks = reinterpret_cast<const Task*>(ctx->tasks[which] + kTaskListHead);
   a.fwd = static_cast<float2*>(ctx->pool);
   a.slot_rows = slot_rows;
-  grid = (int)std::min<int64_t>(grid, (int64_t)tasks.size());
+  const int tiles = scan_tiles_per_cta(ctx->shape);
+  grid = (int)std::min<int64_t>(grid, ceil_div((int64_t)tasks.size(), tiles));
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (ctx->timing) {
     CUDA_TRY(cudaEventCreate(&e0));
     CUDA_TRY(cudaEventCreate(&e1));
     CUDA_TRY(cudaEventRecord(e0, stream));
   }
-  CUDA_TRY(launch_scan(a, grid, ctx->pairs_per_thread, stream));
+  CUDA_TRY(launch_scan(a, grid, ctx->shape, stream));
   ctx->launches++;
   for (const Task& t : tasks) ctx->pair_sites += (double)t.pair_count * (double)(t.ce - t.cs);
   if (ctx->timing) {
@@ -306,10 +336,15 @@ int64_t max_core(const std::vector<Block>& blocks) {
   return m;
 }
 
+// Bytes of one CTA's forward-state slots for a shape.
+size_t cta_slot_bytes(ScanShape shape, int64_t slot_rows) {
+  return (size_t)slot_rows * scan_tile_pairs(shape) * scan_tiles_per_cta(shape) * sizeof(float2);
+}
+
 // Size the forward-state pool for up to `want` CTAs within `budget` bytes;
 // returns the CTA count it can hold (>= 1) or a negative status.
 int size_pool(gsmc_ctx* ctx, int64_t slot_rows, int want, size_t budget, int* grid) {
-  const size_t slot = (size_t)slot_rows * scan_tile_pairs(ctx->pairs_per_thread) * sizeof(float2);
+  const size_t slot = cta_slot_bytes(ctx->shape, slot_rows);
   int64_t g = std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)(budget / std::max<size_t>(slot, 1))));
   int rc = ensure_buffer(reinterpret_cast<char**>(&ctx->pool), &ctx->pool_bytes, (size_t)g * slot);
   if (rc) return rc;
@@ -323,35 +358,37 @@ int run_direct(gsmc_ctx* ctx, const int32_t* d_pi, const int32_t* d_pj, int64_t 
                const std::vector<Block>& blocks, int flags, float* const out[5], int64_t ld,
                int64_t col0, cudaStream_t stream) {
   if (P == 0 || blocks.empty()) return GSMC_OK;
-  const int tile = scan_tile_pairs(ctx->pairs_per_thread);
+  const int tile = scan_tile_pairs(ctx->shape);
   std::vector<Task> tasks;
   tasks.reserve(blocks.size() * ceil_div(P, tile));
   WindowOut wo{{out[0], out[1], out[2], out[3], out[4]}, 0, ld, 0};
   for (const Block& b : blocks)
-    add_window_tasks(b, 0, P, tile, wo, col0, task_flags(flags), 2.0f * ctx->ne, &tasks);
+    add_window_tasks(b, d_pi, d_pj, P, tile, wo, col0, task_flags(flags), 2.0f * ctx->ne, &tasks);
   const size_t budget = (size_t)(0.8 * (double)free_device_bytes()) + ctx->pool_bytes;
+  const int want = (int)std::min<int64_t>(resident_ctas(ctx->shape),
+                                          ceil_div((int64_t)tasks.size(), scan_tiles_per_cta(ctx->shape)));
   int grid = 0;
-  int rc = size_pool(ctx, max_core(blocks), resident_ctas(ctx), budget, &grid);
+  int rc = size_pool(ctx, max_core(blocks), want, budget, &grid);
   if (rc) return rc;
-  return launch_tasks(ctx, tasks, 0, d_pi, d_pj, max_core(blocks), grid, stream);
+  return launch_tasks(ctx, tasks, 0, max_core(blocks), grid, stream);
 }
 
 // Windows x pairs into HOST arrays.  Windows go in groups; each group's
 // launch writes its core rows into one half of a device stage while the
 // copier streams the previous group's half to the host.
 int run_to_host(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int64_t pair_cap,
-                int flags, float* const host[5]) {
+                int flags, float* const host[5], int64_t row0) {
   if (P == 0 || blocks.empty()) return GSMC_OK;
   HostCopier* copier = HostCopier::for_current_device();
   if (!copier) return fail(GSMC_E_CUDA, "CUDA error: no device for the host copier");
   const int nout = n_outputs(flags);
-  const int tile = scan_tile_pairs(ctx->pairs_per_thread);
+  const int tile = scan_tile_pairs(ctx->shape) * scan_tiles_per_cta(ctx->shape);  // pairs per CTA
   const int64_t core = max_core(blocks);
   const int64_t nb = (int64_t)blocks.size();
-  const int resident = resident_ctas(ctx);
+  const int resident = resident_ctas(ctx->shape);
   const size_t budget = (size_t)(0.75 * (double)free_device_bytes()) + ctx->pool_bytes +
                         ctx->stage_bytes;
-  const size_t slot = (size_t)core * tile * sizeof(float2);
+  const size_t slot = cta_slot_bytes(ctx->shape, core);
   // pair chunk and windows per group: enough tasks per launch to fill the GPU
   // twice, within the budget for pool + two stage halves
   int64_t chunk = std::min<int64_t>(P, pair_cap > 0 ? pair_cap : P);
@@ -373,8 +410,10 @@ int run_to_host(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int6
   int rc = ensure_buffer(&ctx->stage, &ctx->stage_bytes, 2 * half * sizeof(float));
   if (rc) return rc;
   const size_t pool_budget = budget > 2 * half * sizeof(float) ? budget - 2 * half * sizeof(float) : slot;
+  // CTAs one launch can keep busy: its (window, pair tile) tasks, at most
+  const int busy = (int)std::min<int64_t>(resident, group * ceil_div(chunk, tile));
   int grid = 0;
-  rc = size_pool(ctx, core, resident, pool_budget, &grid);
+  rc = size_pool(ctx, core, busy, pool_budget, &grid);
   if (rc) return rc;
   for (int i = 0; i < 2; ++i) {
     if (!ctx->stage_free[i]) CUDA_TRY(cudaEventCreateWithFlags(&ctx->stage_free[i], cudaEventDisableTiming));
@@ -404,9 +443,10 @@ int run_to_host(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int6
         wo.off = i * core * n;
         wo.ldo = n;
         wo.row0 = b.cs;
-        add_window_tasks(b, off, n, tile, wo, 0, task_flags(flags), 2.0f * ctx->ne, &tasks);
+        add_window_tasks(b, d_pi + off, d_pj + off, n, scan_tile_pairs(ctx->shape), wo, 0,
+                         task_flags(flags), 2.0f * ctx->ne, &tasks);
       }
-      rc = launch_tasks(ctx, tasks, h, d_pi, d_pj, core, grid, ctx->stream);
+      rc = launch_tasks(ctx, tasks, h, core, grid, ctx->stream);
       if (rc) return rc;
       CUDA_TRY(cudaEventRecord(ctx->launch_done[h], ctx->stream));
       for (int64_t i = 0; i < ng; ++i) {
@@ -415,7 +455,7 @@ int run_to_host(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int6
         for (int k = 0; k < 5; ++k) {
           if (!selected[k]) continue;
           const float* src = base + (size_t)(used++) * group * core * n + (size_t)i * core * n;
-          const int e = copier->enqueue(host[k] + (size_t)b.cs * P + off, (size_t)P * sizeof(float),
+          const int e = copier->enqueue(host[k] + (size_t)(b.cs - row0) * P + off, (size_t)P * sizeof(float),
                                         src, (size_t)n * sizeof(float), (size_t)n * sizeof(float),
                                         (size_t)(b.ce - b.cs), ctx->launch_done[h]);
           if (e != cudaSuccess && !first_err)
@@ -493,7 +533,11 @@ int gsmc_ctx_create(const uint8_t* G, int64_t n_haps, int64_t n_sites, const dou
   ctx->n_groups = (n_sites + 127) / 128;
   if (const char* env = std::getenv("GSMC_PAIRS_PER_THREAD")) {
     const int v = std::atoi(env);
-    if (v == 1 || v == 2) ctx->pairs_per_thread = v;
+    if (v == 1 || v == 2) ctx->shape.pairs_per_thread = v;
+  }
+  if (const char* env = std::getenv("GSMC_SCAN_WIDTH")) {
+    const int v = std::atoi(env);
+    if (v == 32 || v == 128) ctx->shape.width = v;
   }
   int rc = acquire_tables(ctx->device, flow_field_path, (float)Ne, (float)mu, (float)rho, L,
                           &ctx->tables);
@@ -505,7 +549,6 @@ int gsmc_ctx_create(const uint8_t* G, int64_t n_haps, int64_t n_sites, const dou
     }
   } guard{&ctx};
   CUDA_TRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-  CUDA_TRY(cudaMalloc(&ctx->counters, 2 * sizeof(int)));
   const size_t geno_bytes = (size_t)std::max<int64_t>(ctx->n_groups, 1) * std::max<int64_t>(n_haps, 1) * sizeof(ulonglong2);
   CUDA_TRY(cudaMalloc(&ctx->geno, geno_bytes));
   CUDA_TRY(cudaMemsetAsync(ctx->geno, 0, geno_bytes, ctx->stream));
@@ -552,7 +595,6 @@ int gsmc_ctx_destroy(gsmc_ctx* ctx) {
   cudaFree(ctx->pool);
   cudaFree(ctx->pairs);
   cudaFree(ctx->stage);
-  cudaFree(ctx->counters);
   for (int i = 0; i < 2; ++i) {
     cudaFree(ctx->tasks[i]);
     if (ctx->stage_free[i]) cudaEventDestroy(ctx->stage_free[i]);
@@ -635,7 +677,7 @@ static int run_host_common(gsmc_ctx* ctx, const int32_t* pi, const int32_t* pj, 
   float* host[5] = {mean, (flags & GSMC_CI) ? lower : nullptr, (flags & GSMC_CI) ? upper : nullptr,
                     (flags & GSMC_POSTERIOR) ? alpha : nullptr,
                     (flags & GSMC_POSTERIOR) ? beta : nullptr};
-  return run_to_host(ctx, P, blocks, pair_cap, flags, host);
+  return run_to_host(ctx, P, blocks, pair_cap, flags, host, blocks.empty() ? 0 : blocks[0].cs);
 }
 
 int gsmc_run_fb(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j, int64_t n_pairs,
@@ -643,6 +685,19 @@ int gsmc_run_fb(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j, int
   if (int rc = check_ctx(ctx)) return rc;
   std::vector<Block> one;
   if (ctx->n_sites > 0) one.push_back({0, ctx->n_sites, 0, ctx->n_sites});
+  return run_host_common(ctx, pair_i, pair_j, n_pairs, one, -1, flags, mean, lower, upper,
+                         alpha, beta);
+}
+
+int gsmc_run_fb_window(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j,
+                       int64_t n_pairs, int64_t site_begin, int64_t site_end, int flags,
+                       float* mean, float* lower, float* upper, float* alpha, float* beta) {
+  if (int rc = check_ctx(ctx)) return rc;
+  if (site_begin < 0 || site_end > ctx->n_sites || site_begin > site_end)
+    return fail(GSMC_E_INVALID, "site window [%lld, %lld) is out of range for %lld sites",
+                (long long)site_begin, (long long)site_end, (long long)ctx->n_sites);
+  std::vector<Block> one;
+  if (site_end > site_begin) one.push_back({site_begin, site_end, site_begin, site_end});
   return run_host_common(ctx, pair_i, pair_j, n_pairs, one, -1, flags, mean, lower, upper,
                          alpha, beta);
 }

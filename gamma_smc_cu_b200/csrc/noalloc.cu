@@ -1,12 +1,13 @@
 // Allocation-free variant of the device-resident blockwise scan.
 //
-// Some callers cannot let a library allocate device memory during a call:
-// code that runs while a stream is being captured into a CUDA graph (where
-// cudaMalloc/cudaFree are not allowed), frameworks whose own allocator already
-// owns the device memory (a caching allocator or a pre-reserved pool leaves
-// nothing for cudaMalloc), and latency-sensitive services that cannot afford
-// the device-wide synchronisation cudaMalloc/cudaFree imply.  For them this
-// file provides gsmc_run_fb_blockwise_device_noalloc: the same computation as
+// Some callers cannot have a library allocate device memory while they call
+// it: programs whose framework allocator (a caching allocator, or a pool
+// reserved up front) already holds the GPU's memory, so a cudaMalloc would fail
+// or fragment it; services that keep tail latency low and cannot take the
+// device-wide synchronisation cudaMalloc/cudaFree may cause; and host
+// applications that load this library as a plug-in under a device-memory
+// budget of their own.  For them this file provides
+// gsmc_run_fb_blockwise_device_noalloc: the same computation as
 // gsmc_run_fb_blockwise_device, whose only scratch -- the work counter and the
 // per-CTA forward-state slots -- lives in one fixed, file-scope device array
 // instead of in memory allocated at call time.
@@ -49,7 +50,9 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 struct NoAllocArgs {
-  ScanArgs scan;   // genotypes, gap codes, tables and pair indices
+  ScanArgs scan;   // genotypes, gap codes and tables
+  const int32_t* pi;  // pair indices
+  const int32_t* pj;
   int* counter;    // in the scratch, cleared before the launch
   float2* slots;   // in the scratch
   int64_t slot_rows;
@@ -84,7 +87,8 @@ __global__ void __launch_bounds__(kThreads) fb_scan_noalloc(const NoAllocArgs a)
         task.cs = cs;
         task.ce = ce;
         task.pe = min(a.n_sites, ce + a.flank);
-        task.pair_begin = tile * kThreads;
+        task.pi = a.pi + (int64_t)tile * kThreads;
+        task.pj = a.pj + (int64_t)tile * kThreads;
         task.pair_count = min(kThreads, a.n_pairs - tile * kThreads);
         task.out_row0 = 0;
         task.flags = a.flags;
@@ -96,7 +100,7 @@ __global__ void __launch_bounds__(kThreads) fb_scan_noalloc(const NoAllocArgs a)
     }
     __syncthreads();
     if (id >= a.n_tasks) break;
-    scan_task<1>(a.scan, task, slot);
+    scan_task<1, kThreads>(a.scan, task, slot);
   }
 }
 
@@ -179,8 +183,8 @@ extern "C" int gsmc_run_fb_blockwise_device_noalloc(
   a.scan.site_tab = v.site_tab;
   a.scan.chunk_tab = v.chunk_tab;
   a.scan.L = v.L;
-  a.scan.pi = d_pair_i;
-  a.scan.pj = d_pair_j;
+  a.pi = d_pair_i;
+  a.pj = d_pair_j;
   a.counter = reinterpret_cast<int*>(scratch);
   a.slots = reinterpret_cast<float2*>(scratch + kCounterBytes);
   a.slot_rows = core;

@@ -1,7 +1,8 @@
 // Fused Gamma-SMC forward/backward scan for sm_100a.
 //
-// A persistent kernel: every CTA pulls tasks -- up to 128 (x NP) pairs over
-// one padded window -- from a device counter.  Each thread walks its pairs
+// A persistent kernel: every tile of a CTA (one warp, or the whole CTA) pulls
+// tasks -- up to tile width x NP pairs over one padded window -- from a
+// device counter.  Each thread walks its pairs
 // over the window's sites: forward from the padded start to the core end,
 // storing the (m, c) state at core sites in the CTA's slot, then backward from
 // the padded end to the core start, combining with the stored forward state
@@ -35,23 +36,51 @@ namespace {
 #define GSMC_MIN_CTAS 6
 #endif
 
-template <int NP>
+template <int NP, int WIDTH>
 __global__ void __launch_bounds__(kThreads, NP == 1 ? GSMC_MIN_CTAS : GSMC_MIN_CTAS / 2)
     fb_scan_persistent(const ScanArgs a) {
   // The task descriptor lives in shared memory: its fields are uniform across
-  // the CTA and read only where used, so they cost no registers.
-  __shared__ Task task;
-  __shared__ int task_id;
-  float2* slot = a.fwd + (int64_t)blockIdx.x * a.slot_rows * (kThreads * NP);
-  for (;;) {
-    __syncthreads();  // everyone is done with the previous task
-    if (threadIdx.x == 0) {
-      task_id = atomicAdd(a.next_task, 1);
-      if (task_id < a.n_tasks) task = a.tasks[task_id];
+  // the tile and read only where used, so they cost no registers.  (Plain
+  // loads copy it: the list may be mapped host memory.)
+  if constexpr (WIDTH == kThreads) {
+    // the whole CTA takes one task at a time
+    __shared__ Task task;
+    __shared__ int task_id;
+    float2* slot = a.fwd + (int64_t)blockIdx.x * a.slot_rows * (kThreads * NP);
+    for (;;) {
+      __syncthreads();  // everyone is done with the previous task
+      if (threadIdx.x == 0) {
+        // -1 once the list is exhausted (no task count held in registers)
+        const int id = atomicAdd(a.next, 1);
+        task_id = id < *a.count ? id : -1;
+        if (task_id >= 0) task = a.tasks[task_id];
+      }
+      __syncthreads();
+      if (task_id < 0) break;
+      scan_task<NP, kThreads>(a, task, slot);
     }
-    __syncthreads();
-    if (task_id >= a.n_tasks) break;
-    scan_task<NP>(a, task, slot);
+  } else {
+    // each warp takes its own tasks
+    constexpr int kWarps = kThreads / 32;
+    __shared__ Task task[kWarps];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float2* slot = a.fwd + ((int64_t)blockIdx.x * kWarps + w) * a.slot_rows * (32 * NP);
+    for (;;) {
+      __syncwarp();  // the warp is done with the previous task
+      int id = 0;
+      if (lane == 0) {
+        id = atomicAdd(a.next, 1);
+        if (id >= *a.count) id = -1;
+      }
+      id = __shfl_sync(0xffffffffu, id, 0);
+      if (id < 0) break;
+      static_assert(sizeof(Task) % 4 == 0, "Task is copied as 32-bit words");
+      const int* src = reinterpret_cast<const int*>(a.tasks + id);
+      int* dst = reinterpret_cast<int*>(&task[w]);
+      if (lane < (int)(sizeof(Task) / 4)) dst[lane] = src[lane];
+      __syncwarp();
+      scan_task<NP, 32>(a, task[w], slot);
+    }
   }
 }
 
@@ -87,30 +116,55 @@ __global__ void unpack_kernel(const uint64_t* __restrict__ packed, int64_t n, in
 
 int scan_threads() { return kThreads; }
 
-int scan_tile_pairs(int pairs_per_thread) {
-  return kThreads * (pairs_per_thread == 2 ? 2 : 1);
+bool scan_shape_valid(ScanShape shape) {
+  return (shape.width == 32 || shape.width == kThreads) &&
+         (shape.pairs_per_thread == 1 || shape.pairs_per_thread == 2);
 }
 
-int scan_resident_ctas(int pairs_per_thread) {
-  int dev = 0, sms = 0, per_sm = 0;
+int scan_tile_pairs(ScanShape shape) { return shape.width * shape.pairs_per_thread; }
+
+int scan_tiles_per_cta(ScanShape shape) { return kThreads / shape.width; }
+
+namespace {
+
+template <int NP, int WIDTH>
+int resident_of() {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fb_scan_persistent<NP, WIDTH>,
+                                                    kThreads, 0) != cudaSuccess)
+    return 0;
+  return per_sm;
+}
+
+}  // namespace
+
+int scan_resident_ctas(ScanShape shape) {
+  if (!scan_shape_valid(shape)) return 0;
+  int dev = 0, sms = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-  cudaError_t e = pairs_per_thread == 2
-                      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fb_scan_persistent<2>,
-                                                                      kThreads, 0)
-                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fb_scan_persistent<1>,
-                                                                      kThreads, 0);
-  if (e != cudaSuccess) return 0;
+  int per_sm = 0;
+  if (shape.width == 32)
+    per_sm = shape.pairs_per_thread == 2 ? resident_of<2, 32>() : resident_of<1, 32>();
+  else
+    per_sm = shape.pairs_per_thread == 2 ? resident_of<2, kThreads>() : resident_of<1, kThreads>();
   return sms * per_sm;
 }
 
-cudaError_t launch_scan(const ScanArgs& args, int grid, int pairs_per_thread,
-                        cudaStream_t stream) {
-  if (args.n_tasks <= 0 || grid <= 0) return cudaSuccess;
-  if (pairs_per_thread == 2)
-    fb_scan_persistent<2><<<grid, kThreads, 0, stream>>>(args);
-  else
-    fb_scan_persistent<1><<<grid, kThreads, 0, stream>>>(args);
+cudaError_t launch_scan(const ScanArgs& args, int grid, ScanShape shape, cudaStream_t stream) {
+  if (grid <= 0) return cudaSuccess;
+  if (!scan_shape_valid(shape)) return cudaErrorInvalidValue;
+  if (shape.width == 32) {
+    if (shape.pairs_per_thread == 2)
+      fb_scan_persistent<2, 32><<<grid, kThreads, 0, stream>>>(args);
+    else
+      fb_scan_persistent<1, 32><<<grid, kThreads, 0, stream>>>(args);
+  } else {
+    if (shape.pairs_per_thread == 2)
+      fb_scan_persistent<2, kThreads><<<grid, kThreads, 0, stream>>>(args);
+    else
+      fb_scan_persistent<1, kThreads><<<grid, kThreads, 0, stream>>>(args);
+  }
   return cudaGetLastError();
 }
 

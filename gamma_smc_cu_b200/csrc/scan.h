@@ -20,23 +20,33 @@ constexpr int kCodePad = 2;
 // Output selection of a task.
 enum TaskFlags { kTaskCI = 1, kTaskPosterior = 2 };
 
-// One unit of scan work: up to (threads per CTA x pairs per thread) pairs over
-// one padded window.  Forward over [ps, ce), backward over [pe-1 .. cs],
-// posterior at core rows [cs, ce).  Output element (s, pair j of the task) is
+// One unit of scan work: up to (tile width x pairs per thread) pairs over one
+// padded window.  Forward over [ps, ce), backward over [pe-1 .. cs], posterior
+// at core rows [cs, ce).  The task's pairs are (pi[j], pj[j]), j <
+// pair_count.  Output element (s, pair j of the task) is
 // out[k][out_off + (s - out_row0) * ldo + j] for each selected output k
 // (0 mean, 1 lower, 2 upper, 3 alpha, 4 beta).
 struct Task {
   int32_t ps, cs, ce, pe;
-  int32_t pair_begin;   // first pair (index into pi/pj)
-  int32_t pair_count;   // pairs in this task
+  const int32_t* pi;
+  const int32_t* pj;
+  int32_t pair_count;
   int32_t out_row0;
   int32_t flags;        // TaskFlags
+  float unscale;        // 2 * Ne of the task's job
   int64_t out_off;
   int64_t ldo;
   float* out[5];
-  float unscale;        // 2 * Ne of the task's job
-  int32_t pad;
 };
+
+// Head of a device task list: CTAs take task numbers from `next` (zero when
+// the list is uploaded) until it reaches `count`.  Tasks follow at
+// kTaskListHead bytes.
+struct TaskListHead {
+  int next;
+  int count;
+};
+constexpr size_t kTaskListHead = 128;
 
 struct ScanArgs {
   const ulonglong2* geno;   // [n_groups][n_haps]: 128 sites per entry, bit b of .x/.y = site 128g+b / 128g+64+b
@@ -45,26 +55,37 @@ struct ScanArgs {
   const float4* site_tab;   // [2 directions][L][hom, het][2450][2]
   const float4* chunk_tab;  // [2450][2]
   int L;
-  const int32_t* pi;
-  const int32_t* pj;
-  const Task* tasks;
-  int n_tasks;
-  int* next_task;           // work counter, zero at launch
-  float2* fwd;              // per-CTA forward-state slots
+  int* next;                // task counter (device memory, zero at launch)
+  const int* count;         // number of tasks (device or mapped host memory)
+  const Task* tasks;        // the tasks (device or mapped host memory)
+  float2* fwd;              // forward-state slots, one per task slot of the grid
   int64_t slot_rows;        // sites per slot (max core length of the tasks)
 };
 
-// Threads per CTA of the scan and the pairs one thread carries.
+// Launch shape of the scan: `width` threads (32 = one warp, 128 = the whole
+// CTA) share a pair tile and take tasks together; each thread carries
+// `pairs_per_thread` independent pair chains.  A tile holds width x
+// pairs_per_thread pairs and owns one forward-state slot.
+struct ScanShape {
+  int width;             // 32 or 128
+  int pairs_per_thread;  // 1 or 2
+};
+
+// Threads per CTA of the scan kernels.
 int scan_threads();
-int scan_tile_pairs(int pairs_per_thread);
+// Pairs of one task tile and tiles (forward-state slots) per CTA for a shape.
+int scan_tile_pairs(ScanShape shape);
+int scan_tiles_per_cta(ScanShape shape);
+// Whether a shape has a compiled kernel.
+bool scan_shape_valid(ScanShape shape);
 
-// Resident CTAs of the persistent scan kernel on the current device.
-int scan_resident_ctas(int pairs_per_thread);
+// Resident CTAs of the persistent scan kernel of `shape` on the current device.
+int scan_resident_ctas(ScanShape shape);
 
-// Launch the persistent scan over args.n_tasks tasks with `grid` CTAs; each
-// CTA owns forward-state slot blockIdx.x of slot_rows x tile pairs float2.
-cudaError_t launch_scan(const ScanArgs& args, int grid, int pairs_per_thread,
-                        cudaStream_t stream);
+// Launch the persistent scan over the task list of args with `grid`
+// CTAs; CTA b's tile t owns forward-state slot b * tiles_per_cta + t of
+// slot_rows x tile pairs float2.
+cudaError_t launch_scan(const ScanArgs& args, int grid, ScanShape shape, cudaStream_t stream);
 
 // Pack [n_haps x n_sites] uint8 genotypes.  scan_layout: word-major 128-site
 // groups for the scan; otherwise the reference's row-major uint64 words.

@@ -137,15 +137,17 @@ __device__ __forceinline__ void combine_store(const Task& t, int64_t o, float2 f
 constexpr int kFwdPrefetch = 4;
 constexpr int kThreads = 128;
 
-// One task: this thread's NP pairs over the task's padded window.  The
-// forward states live in this CTA's slot, rows of kThreads * NP pairs.
-template <int NP>
+// One task: this thread's NP pairs over the task's padded window.  WIDTH
+// threads (a warp or the whole CTA) share the task; the forward states live in
+// the tile's slot, rows of WIDTH * NP pairs.
+template <int NP, int WIDTH>
 __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, float2* slot) {
-  constexpr int kRow = kThreads * NP;
+  static_assert(WIDTH == 32 || WIDTH == kThreads, "a task is run by one warp or one CTA");
+  constexpr int kRow = WIDTH * NP;
   const int64_t nh = a.n_haps;
   const int ps = t.ps, cs = t.cs, ce = t.ce, pe = t.pe;
   const bool ci = (t.flags & kTaskCI) != 0, post = (t.flags & kTaskPosterior) != 0;
-  const int j0 = threadIdx.x;
+  const int j0 = threadIdx.x & (WIDTH - 1);
   if (j0 >= t.pair_count) return;
 
   const ulonglong2* gi[NP];
@@ -153,12 +155,12 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   bool live[NP];
 #pragma unroll
   for (int k = 0; k < NP; ++k) {
-    const int j = j0 + k * kThreads;
+    const int j = j0 + k * WIDTH;
     int hi = 0, hj = 0;
     live[k] = j < t.pair_count;
     if (live[k]) {
-      hi = a.pi[t.pair_begin + j];
-      hj = a.pj[t.pair_begin + j];
+      hi = t.pi[j];
+      hj = t.pj[j];
       // Device-side pair indices are not validated by the host: a bad pair is
       // skipped (outputs untouched) instead of reading out of bounds.
       if (hi < 0 || hi >= nh || hj < 0 || hj >= nh) {
@@ -223,7 +225,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   }
   if (s >= cs) {
 #pragma unroll
-    for (int k = 0; k < NP; ++k) __stcs(fp + k * kThreads, make_float2(m[k], c[k]));
+    for (int k = 0; k < NP; ++k) __stcs(fp + k * WIDTH, make_float2(m[k], c[k]));
     fp += kRow;
   }
   for (++s; s < cs; ++s) {
@@ -238,7 +240,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     cur = nx;
     nx = nx2;
 #pragma unroll
-    for (int k = 0; k < NP; ++k) __stcs(fp + k * kThreads, make_float2(m[k], c[k]));
+    for (int k = 0; k < NP; ++k) __stcs(fp + k * WIDTH, make_float2(m[k], c[k]));
     fp += kRow;
   }
 
@@ -293,7 +295,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   for (int i = 0; i < kFwdPrefetch; ++i) {
 #pragma unroll
     for (int k = 0; k < NP; ++k)
-      q[i][k] = (ce - 1 - i >= cs) ? __ldlu(fq + k * kThreads) : make_float2(0.0f, 0.0f);
+      q[i][k] = (ce - 1 - i >= cs) ? __ldlu(fq + k * WIDTH) : make_float2(0.0f, 0.0f);
     fq -= kRow;
   }
   int64_t o = t.out_off + (int64_t)(ce - 1 - t.out_row0) * t.ldo + j0;
@@ -311,7 +313,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     const bool ahead = s - kFwdPrefetch >= cs;
 #pragma unroll
     for (int k = 0; k < NP; ++k)
-      q[kFwdPrefetch - 1][k] = ahead ? __ldlu(fq + k * kThreads) : make_float2(0.0f, 0.0f);
+      q[kFwdPrefetch - 1][k] = ahead ? __ldlu(fq + k * WIDTH) : make_float2(0.0f, 0.0f);
     fq -= kRow;
     const SiteCode sc = cur;
     const SiteCode nx2 = code[s - 2];
@@ -326,7 +328,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     if (more) bwd_fetch(s, sc, nx.layer, fe);
 #pragma unroll
     for (int k = 0; k < NP; ++k)
-      if (live[k]) combine_store(t, o + k * kThreads, f[k], mb[k], cb[k], ci, post);
+      if (live[k]) combine_store(t, o + k * WIDTH, f[k], mb[k], cb[k], ci, post);
     o -= t.ldo;
     if (more) bwd_finish(sc, fe);
     cur = nx;

@@ -1,0 +1,267 @@
+"""Continuous-batching TMRCA query server over one resident context.
+
+A query asks for the posterior of a pair subset over a region (a site range,
+or a base-pair range mapped to sites through the positions) and gets back the
+same result dict ``FlowContext.run_fb_window`` returns for it.  Queries arrive
+at any time from any thread (``submit`` returns a ``concurrent.futures.Future``).
+
+The scheduler thread keeps several batches in flight, each on its own
+executor (its own forward-state pool and task list) and CUDA stream.  As soon
+as an executor is free it admits every waiting query that fits -- into the
+device-memory budget for outputs (free HBM measured at start-up, minus
+headroom) and the batch's task capacity -- and launches them together as one
+persistent kernel, followed by the device-to-host copy of their outputs on
+the same stream.  Queries that arrive while earlier batches are on the GPU
+therefore start as soon as an executor and memory free up, and their work
+overlaps the tail of the running batches on the device.  Genotypes, gap codes
+and flow-field tables stay resident in the context the whole time.
+
+A query whose outputs alone exceed the whole budget is rejected with
+MemoryError; malformed queries are rejected at ``submit`` with ValueError.
+``stats()`` reports latency percentiles (arrival to result), throughput and
+admission counters.
+"""
+from __future__ import annotations
+
+import collections
+import threading
+import time
+from concurrent.futures import Future
+
+import numpy as np
+
+from .batch import DeviceBatch, Executor, Job, Layout, _count_tasks, validate
+
+BYTES_PER_FLOAT = 4
+
+
+def _new_stream(device):
+    import torch
+    return torch.cuda.Stream(device)
+
+
+def _free_device_bytes(device):
+    import torch
+    return torch.cuda.mem_get_info(device)[0]
+
+
+def _bind_thread(device):
+    import torch
+    if torch.cuda.is_available():
+        torch.cuda.set_device(device)
+
+
+class _Request:
+    __slots__ = ("job", "future", "t_arrive", "t_admit", "t_done", "bytes", "tasks")
+
+    def __init__(self, job, future, t_arrive, nbytes, tasks):
+        self.job = job
+        self.future = future
+        self.t_arrive = t_arrive
+        self.t_admit = None
+        self.t_done = None
+        self.bytes = nbytes
+        self.tasks = tasks
+
+
+class _Slot:
+    """One executor, its stream, and the batch it is running (if any)."""
+
+    def __init__(self, executor, stream):
+        self.executor = executor
+        self.stream = stream
+        self.batch = None
+        self.requests = []
+        self.bytes = 0
+
+
+class TmrcaServer:
+    """Request loop with continuous batching over ``ctx`` (a FlowContext).
+
+    ``positions`` (site coordinates) enables base-pair regions.
+    ``max_inflight`` executors run concurrently; ``core_block_sites`` /
+    ``flank_sites`` chunk long windows (0 = whole windows), ``tile_width`` /
+    ``pairs_per_thread`` set the launch shape (see :mod:`.tune` for picking
+    them); ``hbm_budget`` bounds the device bytes of in-flight outputs
+    (default: half the free device memory after the executors exist).
+    """
+
+    def __init__(self, ctx, positions=None, max_inflight=3, core_block_sites=4096,
+                 flank_sites=2048, tile_width=128, pairs_per_thread=1, use_graph=True,
+                 hbm_budget=None, max_tasks=1 << 15, max_batch_requests=4096,
+                 poll_interval=50e-6):
+        self.ctx = ctx
+        self.positions = None if positions is None else np.asarray(positions, np.float64)
+        self.device = ctx.device_id
+        self.config = {"tile_width": tile_width, "pairs_per_thread": pairs_per_thread,
+                       "core_block_sites": core_block_sites, "flank_sites": flank_sites,
+                       "use_graph": use_graph, "max_tasks": max_tasks}
+        if core_block_sites <= 0:
+            self.config["max_window_sites"] = ctx.n_sites
+        # looked up on the module at call time, so host-side tests can
+        # substitute fakes for the device pieces
+        self.slots = [_Slot(Executor(ctx, **self.config), _new_stream(self.device))
+                      for _ in range(max(1, int(max_inflight)))]
+        if hbm_budget is None:
+            hbm_budget = int(0.5 * _free_device_bytes(self.device))
+        self.hbm_budget = int(hbm_budget)
+        self.max_tasks = int(max_tasks)
+        self.max_batch_requests = int(max_batch_requests)
+        self.poll_interval = float(poll_interval)
+        self._pending = collections.deque()
+        self._cv = threading.Condition()
+        self._closing = False
+        self._in_use = 0
+        self._done = []           # finished requests (for stats)
+        self.counters = collections.Counter()
+        self._thread = threading.Thread(target=self._loop, name="gsmc-serve", daemon=True)
+        self._thread.start()
+
+    # ------------------------------------------------------------ client API
+
+    def sites_of(self, start_bp, end_bp):
+        """Site range [s0, s1) of the sites with start_bp <= position < end_bp."""
+        if self.positions is None:
+            raise ValueError("the server has no positions; give site ranges")
+        s0 = int(np.searchsorted(self.positions, start_bp, side="left"))
+        s1 = int(np.searchsorted(self.positions, end_bp, side="left"))
+        return s0, max(s0, s1)
+
+    def submit(self, pairs, site_begin=None, site_end=None, region_bp=None, mean_only=True,
+               return_posterior=False):
+        """Queue one query; returns a Future of its result dict."""
+        if region_bp is not None:
+            site_begin, site_end = self.sites_of(*region_bp)
+        if site_begin is None:
+            site_begin = 0
+        if site_end is None:
+            site_end = self.ctx.n_sites
+        job = Job(pairs, site_begin, site_end, mean_only=mean_only,
+                  return_posterior=return_posterior)
+        validate(job, self.ctx.n_haps, self.ctx.n_sites)
+        fut = Future()
+        req = _Request(job, fut, time.perf_counter(), job.output_floats * BYTES_PER_FLOAT,
+                       _count_tasks([job], self.config))
+        with self._cv:
+            if self._closing:
+                raise RuntimeError("server is closed")
+            self._pending.append(req)
+            self.counters["submitted"] += 1
+            self._cv.notify()
+        return fut
+
+    def close(self, wait=True):
+        with self._cv:
+            self._closing = True
+            self._cv.notify()
+        if wait:
+            self._thread.join()
+        for s in self.slots:
+            s.executor.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def stats(self, reset=False):
+        """Latency percentiles (ms), throughput and counters of finished queries."""
+        with self._cv:
+            done = list(self._done)
+            counters = dict(self.counters)
+            if reset:
+                self._done.clear()
+                self.counters.clear()
+        out = {"completed": len(done), **counters}
+        if done:
+            lat = np.array([r.t_done - r.t_arrive for r in done]) * 1e3
+            queue = np.array([r.t_admit - r.t_arrive for r in done]) * 1e3
+            span = max(r.t_done for r in done) - min(r.t_arrive for r in done)
+            ps = float(sum(r.job.pair_sites for r in done))
+            out.update({"p50_ms": float(np.percentile(lat, 50)),
+                        "p99_ms": float(np.percentile(lat, 99)),
+                        "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
+                        "queue_p50_ms": float(np.percentile(queue, 50)),
+                        "pair_sites": ps, "span_s": span,
+                        "pair_sites_per_s": ps / span if span > 0 else None})
+        return out
+
+    # ------------------------------------------------------------- scheduler
+
+    def _finish(self, slot):
+        results = slot.batch.layout.results(slot.batch.h_out.numpy())
+        now = time.perf_counter()
+        for req, res in zip(slot.requests, results):
+            req.t_done = now
+            # copy out of the pinned buffer so it can be reused
+            req.future.set_result({k: np.array(v) for k, v in res.items()})
+        with self._cv:
+            self._in_use -= slot.bytes
+            self._done.extend(slot.requests)
+            self.counters["batches"] += 1
+        slot.batch = None
+        slot.requests = []
+        slot.bytes = 0
+
+    def _admit(self, slot):
+        """Move the waiting queries that fit into a new batch on ``slot``."""
+        take, nbytes, ntasks = [], 0, 0
+        with self._cv:
+            while self._pending and len(take) < self.max_batch_requests:
+                req = self._pending[0]
+                if req.bytes > self.hbm_budget or req.tasks > self.max_tasks:
+                    self._pending.popleft()
+                    self.counters["rejected"] += 1
+                    req.future.set_exception(MemoryError(
+                        f"query needs {req.bytes} bytes of outputs and {req.tasks} tasks; the "
+                        f"server holds at most {self.hbm_budget} bytes and {self.max_tasks} "
+                        "tasks per batch"))
+                    continue
+                if (self._in_use + nbytes + req.bytes > self.hbm_budget
+                        or ntasks + req.tasks > self.max_tasks):
+                    break
+                self._pending.popleft()
+                take.append(req)
+                nbytes += req.bytes
+                ntasks += req.tasks
+            if not take:
+                return False
+            self._in_use += nbytes
+            self.counters["admitted"] += len(take)
+        now = time.perf_counter()
+        for r in take:
+            r.t_admit = now
+        try:
+            batch = DeviceBatch(Layout([r.job for r in take]), self.device)
+            batch.launch(slot.executor, slot.stream)
+        except Exception as e:  # a launch failure fails the batch's queries
+            with self._cv:
+                self._in_use -= nbytes
+                self.counters["failed"] += len(take)
+            for r in take:
+                r.future.set_exception(e)
+            return True
+        slot.batch, slot.requests, slot.bytes = batch, take, nbytes
+        return True
+
+    def _loop(self):
+        _bind_thread(self.device)
+        while True:
+            busy = False
+            for slot in self.slots:
+                if slot.batch is not None and slot.batch.done.query():
+                    self._finish(slot)
+                    busy = True
+            for slot in self.slots:
+                if slot.batch is None and self._pending:
+                    busy |= self._admit(slot)
+            with self._cv:
+                idle = all(s.batch is None for s in self.slots)
+                if self._closing and not self._pending and idle:
+                    return
+                if not busy:
+                    if idle and not self._pending:
+                        self._cv.wait(timeout=0.05)
+                    else:
+                        self._cv.wait(timeout=self.poll_interval)

@@ -118,3 +118,52 @@ def cohort(name, n_sites=None):
     if n_sites is not None:
         pos = pos[:n_sites]
     return haplotypes(n, pos, sg), pos
+
+
+def _log_uniform_int(rng, lo, hi, size=None):
+    return np.rint(np.exp(rng.uniform(np.log(lo), np.log(hi), size))).astype(np.int64)
+
+
+def _distinct_pairs(rng, n_haps, n):
+    total = n_haps * (n_haps - 1) // 2
+    return pairs_from_index(np.sort(rng.choice(total, size=min(n, total), replace=False)))
+
+
+def job_mix(n_haps, n_sites, n_jobs=512, seed=5, pairs_range=(1, 4096),
+            window_range=(1_000, 200_000)):
+    """Uneven batch of jobs: pair count log-uniform in pairs_range (random
+    distinct pairs), window length in sites log-uniform in window_range at a
+    uniform random start; both clamped to the cohort.  Returns dicts with
+    pairs / site_begin / site_end (mean_only)."""
+    rng = np.random.default_rng(seed)
+    n_p = _log_uniform_int(rng, pairs_range[0], pairs_range[1], n_jobs)
+    n_w = _log_uniform_int(rng, window_range[0], window_range[1], n_jobs)
+    jobs = []
+    for p, w in zip(n_p, n_w):
+        w = int(min(max(1, w), n_sites))
+        s0 = int(rng.integers(0, n_sites - w + 1))
+        jobs.append({"pairs": _distinct_pairs(rng, n_haps, int(max(1, p))), "site_begin": s0,
+                     "site_end": s0 + w})
+    return jobs
+
+
+def request_stream(positions, n_haps, n_requests, rate, seed=6, pairs_range=(1, 8192),
+                   region_bp=(1_000, 5_000_000), posterior_fraction=0.2):
+    """Poisson stream of TMRCA queries: arrival times (s) at ``rate`` per
+    second, pair subsets of log-uniform size (random distinct pairs, clamped
+    to the cohort), regions of log-uniform length in base pairs at a uniform
+    start (clamped to the sequence), a ``posterior_fraction`` of them asking
+    for the full posterior (mean + alpha + beta), the rest mean-only.
+    Returns dicts with t / pairs / region_bp / mean_only / return_posterior."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n_requests)) if rate > 0 else np.zeros(n_requests)
+    lo, hi = float(positions[0]), float(positions[-1]) + 1.0
+    out = []
+    for k in range(n_requests):
+        n = int(max(1, _log_uniform_int(rng, pairs_range[0], pairs_range[1])))
+        length = float(min(hi - lo, np.exp(rng.uniform(np.log(region_bp[0]), np.log(region_bp[1])))))
+        a = float(rng.uniform(lo, hi - length)) if hi - length > lo else lo
+        post = bool(rng.random() < posterior_fraction)
+        out.append({"t": float(t[k]), "pairs": _distinct_pairs(rng, n_haps, n),
+                    "region_bp": (a, a + length), "mean_only": True, "return_posterior": post})
+    return out

@@ -93,6 +93,20 @@ int gsmc_run_fb(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j,
                 int64_t n_pairs, int flags, float* mean, float* lower,
                 float* upper, float* alpha, float* beta);
 
+/*
+ * Forward/backward over one window [site_begin, site_end) of the context's
+ * sites into HOST arrays of [site_end - site_begin x n_pairs] float32.  The
+ * window is decoded as the reference's block kernels decode a padded window:
+ * the scan restarts at (m, c) = (0, 0) and a window that does not start at
+ * site 0 enters its first site by one base pair.  [0, n_sites) is run_fb.
+ * Replaces one window of gamma_smc_flow_cached_fb_block_gpu
+ * (src/kernels/gamma_smc_flow.cu:632-669, 762-839, 970-997) driven like
+ * FlowContext::run_fb (src/bindings.cpp:2897-2989); a per-request query.
+ */
+int gsmc_run_fb_window(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j,
+                       int64_t n_pairs, int64_t site_begin, int64_t site_end, int flags,
+                       float* mean, float* lower, float* upper, float* alpha, float* beta);
+
 /* Number of windows make_block_windows yields for (n_sites, core_block_sites). */
 int gsmc_block_count(int64_t n_sites, int64_t core_block_sites, int64_t* n_blocks);
 
@@ -132,9 +146,10 @@ int gsmc_run_fb_blockwise_device(gsmc_ctx* ctx, const int32_t* d_pair_i,
 
 /*
  * Same as gsmc_run_fb_blockwise_device, but the call allocates no device
- * memory: for callers that cannot allocate during the call (inside CUDA graph
- * stream capture, under a framework allocator that owns the device memory,
- * or in latency-bound loops that cannot pay for cudaMalloc's device sync).
+ * memory: for callers that cannot have it allocate (a framework allocator
+ * that already holds the GPU's memory, a service that cannot take the
+ * device-wide synchronisation cudaMalloc/cudaFree may cause, a host
+ * application with its own device-memory budget for plug-ins).
  * Its scratch is a fixed 128 MiB device array held by every GPU that loads
  * the library until exit; core_block_sites above 131,071 (one CTA slot no
  * longer fits) is rejected with GSMC_E_INVALID.  All calls share that array:
@@ -148,6 +163,65 @@ int gsmc_run_fb_blockwise_device_noalloc(gsmc_ctx* ctx, const int32_t* d_pair_i,
                                          int flags, float* d_mean, float* d_lower,
                                          float* d_upper, float* d_alpha, float* d_beta,
                                          int64_t ld_out, int64_t out_col0, void* stream);
+
+/* ------------------------------------------------------------ batching --
+ * Many jobs -- each a pair set over a site window with its own outputs -- in
+ * one persistent launch.  No reference counterpart: the reference launches
+ * one kernel pair per call and per block (src/bindings.cpp:3094-3201).
+ */
+typedef struct gsmc_exec gsmc_exec;
+
+typedef struct gsmc_exec_config {
+  int32_t tile_width;        /* threads sharing a pair tile: 32 (a warp) or 128 (a CTA); 0 = 32 */
+  int32_t pairs_per_thread;  /* independent pair chains per thread: 1 or 2; 0 = 1 */
+  int64_t core_block_sites;  /* sites per chunk of a job window; <= 0 = whole windows */
+  int64_t flank_sites;       /* burn-in sites on each side of a chunk; < 0 = 2048 */
+  int64_t max_window_sites;  /* longest window with core_block_sites <= 0; 0 = n_sites */
+  int64_t max_tasks;         /* (chunk, pair tile) tasks per run; 0 = 65536 */
+  uint64_t max_pool_bytes;   /* forward-state pool cap; 0 = half of the free device memory */
+  int32_t max_ctas;          /* cap on the persistent grid; 0 = every resident CTA */
+  int32_t use_graph;         /* 1 = replay upload + launch as one CUDA graph */
+} gsmc_exec_config;
+
+typedef struct gsmc_job {
+  const int32_t* pair_i;     /* DEVICE [n_pairs] haplotype indices */
+  const int32_t* pair_j;
+  int64_t n_pairs;
+  int64_t site_begin;        /* window [site_begin, site_end) of the context's sites */
+  int64_t site_end;
+  int32_t flags;             /* GSMC_CI | GSMC_POSTERIOR */
+  int32_t reserved;
+  float* out[5];             /* DEVICE mean, lower, upper, alpha, beta: element (s, p) at
+                                out[k][(s - site_begin) * ld_out + out_col0 + p] */
+  int64_t ld_out;
+  int64_t out_col0;
+} gsmc_job;
+
+/*
+ * Create an executor: the forward-state pool, device task list and pinned
+ * upload buffers of one in-flight launch (all scratch, allocated here once).
+ * cfg may be NULL for defaults.  Several executors of one context may run
+ * concurrently on different streams; one executor's runs must be ordered on
+ * one stream.
+ */
+int gsmc_exec_create(gsmc_ctx* ctx, const gsmc_exec_config* cfg, gsmc_exec** out);
+int gsmc_exec_destroy(gsmc_exec* exec);
+int gsmc_exec_info(const gsmc_exec* exec, int* grid, uint64_t* pool_bytes, int64_t* slot_rows,
+                   int64_t* max_tasks);
+
+/*
+ * Enqueue all jobs as one persistent launch on `stream` and return.  Each
+ * job's window is decoded as by gsmc_run_fb_window, cut into chunks of
+ * core_block_sites with flank_sites of burn-in when the executor chunks.
+ * Device pair indices are not validated on the host: out-of-range pairs are
+ * skipped on the device and their output columns left unwritten.
+ */
+int gsmc_exec_run(gsmc_exec* exec, const gsmc_job* jobs, int64_t n_jobs, void* stream);
+
+/* Kernel timing of an executor's launches (as gsmc_ctx_timing). */
+int gsmc_exec_timing(gsmc_exec* exec, int enable);
+int gsmc_exec_timing_read(gsmc_exec* exec, double* kernel_ms, int64_t* launches,
+                          double* pair_sites);
 
 /* Bytes of device scratch the context currently holds (forward-state pool). */
 int gsmc_ctx_scratch_bytes(const gsmc_ctx* ctx, uint64_t* bytes);

@@ -1,10 +1,11 @@
 """GPU test of the allocation-free entry point.
 
-gsmc_run_fb_blockwise_device_noalloc serves callers that must not have the
-library allocate device memory during a call -- code running under CUDA graph
-stream capture, programs whose framework allocator already owns the device
-memory, and latency-bound loops that cannot pay for cudaMalloc's device-wide
-synchronisation.  Its scratch is a fixed device array inside the library.
+gsmc_run_fb_blockwise_device_noalloc serves callers that cannot have the
+library allocate device memory during a call: programs whose framework
+allocator already holds the GPU's memory, services that cannot take the
+device-wide synchronisation cudaMalloc/cudaFree may cause, and host
+applications that load the library as a plug-in under their own
+device-memory budget.  Its scratch is a fixed device array inside the library.
 
 This file is named so that pytest collects it last: if it fails, a run that
 stops at the first failure has already run every other test.  It builds all

@@ -98,6 +98,8 @@ SIGNATURES = {
     "gsmc_exec_timing": (c_int, [c_vp, c_int]),
     "gsmc_exec_timing_read": (c_int, [c_vp, ctypes.POINTER(ctypes.c_double), c_i64p,
                                       ctypes.POINTER(ctypes.c_double)]),
+    "gsmc_copy_to_host": (c_int, [c_i64, ctypes.POINTER(c_vp), ctypes.POINTER(c_vp), c_u64p,
+                                  c_vp]),
     "gsmc_ctx_scratch_bytes": (c_int, [c_vp, c_u64p]),
     "gsmc_ctx_timing": (c_int, [c_vp, c_int]),
     "gsmc_ctx_timing_read": (c_int, [c_vp, ctypes.POINTER(ctypes.c_double), c_i64p,

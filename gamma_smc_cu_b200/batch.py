@@ -87,6 +87,15 @@ def validate(job, n_haps, n_sites):
         raise ValueError(f"pair index out of range for {n_haps} haplotypes")
 
 
+# numpy image of gsmc_job (include/gsmc_b200.h), so a batch's descriptors are
+# built with array operations instead of one ctypes field at a time
+JOB_DTYPE = np.dtype([("pair_i", "<u8"), ("pair_j", "<u8"), ("n_pairs", "<i8"),
+                      ("site_begin", "<i8"), ("site_end", "<i8"), ("flags", "<i4"),
+                      ("reserved", "<i4"), ("out", "<u8", (5,)), ("ld_out", "<i8"),
+                      ("out_col0", "<i8")])
+_ALIGN = 64  # floats: every output region starts on a 256-byte boundary
+
+
 class Layout:
     """Where each job's pairs and outputs sit in one flat batch buffer.
 
@@ -97,58 +106,69 @@ class Layout:
 
     def __init__(self, jobs):
         self.jobs = list(jobs)
-        self.pair_off = []
-        self.out_off = []
-        po = 0
-        oo = 0
-        for j in self.jobs:
-            self.pair_off.append(po)
-            po += 2 * j.n_pairs
-            offs = []
-            for sel in _selected(j.mean_only, j.return_posterior):
-                if sel:
-                    offs.append(oo)
-                    oo += -(-j.rows * j.n_pairs // 64) * 64
-                else:
-                    offs.append(None)
-            self.out_off.append(offs)
-        self.pair_ints = po
-        self.out_floats = oo
+        J = len(self.jobs)
+        n = np.fromiter((j.n_pairs for j in self.jobs), np.int64, J)
+        rows = np.fromiter((j.rows for j in self.jobs), np.int64, J)
+        sel = np.array([_selected(j.mean_only, j.return_posterior) for j in self.jobs],
+                       dtype=bool).reshape(J, 5)
+        self.n_pairs, self.rows, self.sel = n, rows, sel
+        self.pair_off = np.concatenate([[0], np.cumsum(2 * n)[:-1]]) if J else n
+        size = -(-(rows * n) // _ALIGN) * _ALIGN
+        sizes = np.where(sel, size[:, None], 0).ravel()
+        offs = np.concatenate([[0], np.cumsum(sizes)[:-1]]) if J else sizes
+        self.out_off = np.where(sel.ravel(), offs, -1).reshape(J, 5)
+        self.pair_ints = int(2 * n.sum())
+        self.out_floats = int(sizes.sum())
+        self.flags = np.fromiter((j.flags for j in self.jobs), np.int32, J)
 
     def pack_pairs(self, dst):
         """Write every job's pairs into the int32 array ``dst``."""
-        for j, o in zip(self.jobs, self.pair_off):
-            n = j.n_pairs
-            dst[o:o + n] = j.pairs[:, 0]
-            dst[o + n:o + 2 * n] = j.pairs[:, 1]
+        if self.jobs:
+            parts = [p for j in self.jobs for p in (j.pairs[:, 0], j.pairs[:, 1])]
+            dst[:self.pair_ints] = np.concatenate(parts)
+
+    def job_array(self, pair_base, out_base):
+        """gsmc_job records (JOB_DTYPE) for device buffers at the given addresses."""
+        J = len(self.jobs)
+        a = np.zeros(J, JOB_DTYPE)
+        a["pair_i"] = pair_base + 4 * self.pair_off
+        a["pair_j"] = pair_base + 4 * (self.pair_off + self.n_pairs)
+        a["n_pairs"] = self.n_pairs
+        a["site_begin"] = [j.site_begin for j in self.jobs]
+        a["site_end"] = [j.site_end for j in self.jobs]
+        a["flags"] = self.flags
+        a["out"] = np.where(self.out_off >= 0, out_base + 4 * self.out_off, 0).astype(np.uint64)
+        a["ld_out"] = self.n_pairs
+        return a
 
     def c_jobs(self, pair_base, out_base):
-        """ctypes gsmc_job array for device buffers at the given addresses."""
-        arr = (_lib.Job * len(self.jobs))()
-        for k, (j, po, offs) in enumerate(zip(self.jobs, self.pair_off, self.out_off)):
-            c = arr[k]
-            c.pair_i = pair_base + 4 * po
-            c.pair_j = pair_base + 4 * (po + j.n_pairs)
-            c.n_pairs = j.n_pairs
-            c.site_begin = j.site_begin
-            c.site_end = j.site_end
-            c.flags = j.flags
-            for i, o in enumerate(offs):
-                c.out[i] = None if o is None else out_base + 4 * o
-            c.ld_out = j.n_pairs
-            c.out_col0 = 0
+        """ctypes view (gsmc_job array) of job_array; keeps the array alive."""
+        a = self.job_array(pair_base, out_base)
+        arr = (_lib.Job * len(self.jobs)).from_buffer(a)
+        arr._keep = a
         return arr
 
     def results(self, host):
         """Per-job result dicts of views into the float32 host array."""
         res = []
-        for j, offs in zip(self.jobs, self.out_off):
+        for k, j in enumerate(self.jobs):
             d = {}
-            for key, o in zip(OUTPUT_KEYS, offs):
-                if o is not None:
+            for i, key in enumerate(OUTPUT_KEYS):
+                o = int(self.out_off[k, i])
+                if o >= 0:
                     d[key] = host[o:o + j.rows * j.n_pairs].reshape(j.rows, j.n_pairs)
             res.append(d)
         return res
+
+    def regions(self):
+        """(job index, output key, float offset, floats) of every output."""
+        out = []
+        for k, j in enumerate(self.jobs):
+            for i, key in enumerate(OUTPUT_KEYS):
+                o = int(self.out_off[k, i])
+                if o >= 0 and j.rows * j.n_pairs:
+                    out.append((k, key, o, j.rows * j.n_pairs))
+        return out
 
 
 class Executor:
@@ -216,7 +236,14 @@ class Executor:
 
 
 class DeviceBatch:
-    """Device (and pinned host) buffers of one batch of jobs."""
+    """Device buffers of one batch of jobs, and where its results go.
+
+    ``launch`` uploads the pairs, runs the jobs and -- when ``host`` is given
+    (a pinned float32 array of ``layout.out_floats``) -- copies every output
+    into it on the same stream.  Without ``host`` the outputs stay on the
+    device; ``to_host`` then copies them into fresh (pageable) numpy arrays
+    through the library's pinned ring.
+    """
 
     def __init__(self, layout, device):
         import torch
@@ -228,6 +255,7 @@ class DeviceBatch:
         self.d_out = None
         self.h_out = None
         self.done = None
+        self.stream = None
 
     def allocate(self, stream):
         """Device buffers, allocated on the stream that will use them."""
@@ -238,26 +266,56 @@ class DeviceBatch:
             self.d_out = torch.empty(max(self.layout.out_floats, 1), dtype=torch.float32,
                                      device=self.device)
 
-    def launch(self, executor, stream):
-        """Upload pairs, run the jobs, copy every output back to pinned host
-        memory, all on ``stream``; returns the completion event."""
+    def launch(self, executor, stream, host=None):
+        """Upload pairs, run the jobs, optionally copy the outputs into the
+        pinned array ``host``; all on ``stream``.  Returns the completion event."""
         import torch
         if self.d_out is None:
             self.allocate(stream)
+        self.stream = stream
         with torch.cuda.stream(stream):
             self.d_pairs.copy_(self.h_pairs, non_blocking=True)
             executor.run(self.layout, self.d_pairs.data_ptr(), self.d_out.data_ptr(),
                          stream.cuda_stream)
-            self.h_out = torch.empty(self.d_out.numel(), dtype=torch.float32, pin_memory=True)
-            self.h_out.copy_(self.d_out, non_blocking=True)
+            if host is not None:
+                self.h_out = host
+                n = self.layout.out_floats
+                if n:
+                    torch.from_numpy(host[:n]).copy_(self.d_out[:n], non_blocking=True)
             self.done = torch.cuda.Event()
             self.done.record(stream)
         return self.done
 
     def results(self):
-        """Per-job result dicts (views into the pinned host buffer); waits."""
+        """Per-job result dicts (views into the pinned host array); waits."""
+        if self.h_out is None:
+            raise RuntimeError("the batch was launched without a host array; use to_host()")
         self.done.synchronize()
-        return self.layout.results(self.h_out.numpy())
+        return self.layout.results(self.h_out)
+
+    def to_host(self):
+        """Per-job result dicts of new numpy arrays, copied from the device
+        outputs once the batch is done (no pinned staging of the results)."""
+        res = [{} for _ in self.layout.jobs]
+        regs = self.layout.regions()
+        dst, src, nb = [], [], []
+        base = self.d_out.data_ptr()
+        for k, key, off, n in regs:
+            j = self.layout.jobs[k]
+            a = np.empty((j.rows, j.n_pairs), np.float32)
+            res[k][key] = a
+            dst.append(a.ctypes.data)
+            src.append(base + 4 * off)
+            nb.append(4 * n)
+        for k, j in enumerate(self.layout.jobs):   # empty outputs
+            for i, key in enumerate(OUTPUT_KEYS):
+                if self.layout.out_off[k, i] >= 0 and key not in res[k]:
+                    res[k][key] = np.empty((j.rows, j.n_pairs), np.float32)
+        m = len(dst)
+        check(_lib.load().gsmc_copy_to_host(
+            m, (ctypes.c_void_p * max(m, 1))(*dst), (ctypes.c_void_p * max(m, 1))(*src),
+            (ctypes.c_uint64 * max(m, 1))(*nb), self.stream.cuda_stream))
+        return res
 
 
 def run_jobs(ctx, jobs, executor=None, stream=None, **config):
@@ -279,7 +337,7 @@ def run_jobs(ctx, jobs, executor=None, stream=None, **config):
         stream = stream or torch.cuda.current_stream(device)
         b = DeviceBatch(Layout(jobs), device)
         b.launch(executor, stream)
-        return b.results()
+        return b.to_host()
     finally:
         if own:
             executor.close()

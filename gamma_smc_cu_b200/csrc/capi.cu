@@ -154,8 +154,10 @@ struct gsmc_ctx {
   size_t pool_bytes = 0;
   int32_t* pairs = nullptr;  // host-path pair indices: [pi | pj]
   int64_t pairs_cap = 0;
-  float* stage = nullptr;  // host-path output stage: two halves
+  float* stage = nullptr;  // host-path output stage: two halves (or summary partials)
   size_t stage_bytes = 0;
+  void* acc = nullptr;     // summary accumulators: double sum, float min, max, mean per site
+  size_t acc_bytes = 0;
   unsigned char* tasks[2] = {nullptr, nullptr};  // task lists of alternating launches
   size_t tasks_cap[2] = {0, 0};                  // bytes
   cudaEvent_t stage_free[2] = {nullptr, nullptr};
@@ -320,7 +322,8 @@ int launch_tasks(gsmc_ctx* ctx, std::vector<Task>& tasks, int which, int64_t slo
     CUDA_TRY(cudaEventCreate(&e1));
     CUDA_TRY(cudaEventRecord(e0, stream));
   }
-  CUDA_TRY(launch_scan(a, grid, ctx->shape, stream));
+  const bool summary = (tasks.front().flags & kTaskSummary) != 0;
+  CUDA_TRY(launch_scan(a, grid, ctx->shape, stream, summary));
   ctx->launches++;
   for (const Task& t : tasks) ctx->pair_sites += (double)t.pair_count * (double)(t.ce - t.cs);
   if (ctx->timing) {
@@ -595,6 +598,7 @@ int gsmc_ctx_destroy(gsmc_ctx* ctx) {
   cudaFree(ctx->pool);
   cudaFree(ctx->pairs);
   cudaFree(ctx->stage);
+  cudaFree(ctx->acc);
   for (int i = 0; i < 2; ++i) {
     cudaFree(ctx->tasks[i]);
     if (ctx->stage_free[i]) cudaEventDestroy(ctx->stage_free[i]);
@@ -689,6 +693,85 @@ int gsmc_run_fb(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j, int
                          alpha, beta);
 }
 
+int gsmc_run_fb_summary(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j,
+                        int64_t n_pairs, int64_t core_block_sites, int64_t flank_sites,
+                        float* site_mean, float* site_min, float* site_max) {
+  if (int rc = check_ctx(ctx)) return rc;
+  if (n_pairs < 0) return fail(GSMC_E_INVALID, "negative pair count");
+  if (flank_sites < 0) return fail(GSMC_E_INVALID, "flank_sites must be non-negative.");
+  const int64_t S = ctx->n_sites;
+  if (n_pairs == 0 || S == 0) return GSMC_OK;
+  if (!pair_i || !pair_j) return fail(GSMC_E_INVALID, "null pair arrays");
+  if (!site_mean || !site_min || !site_max) return fail(GSMC_E_INVALID, "null summary output");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  int rc = upload_pairs(ctx, pair_i, pair_j, n_pairs);
+  if (rc) return rc;
+  std::vector<Block> blocks;
+  if (core_block_sites <= 0 || core_block_sites >= S)
+    blocks.push_back({0, S, 0, S});
+  else
+    blocks = make_windows(S, core_block_sites, flank_sites);
+  const int64_t core = max_core(blocks);
+  const int tile = scan_tile_pairs(ctx->shape);
+  const int warps = ctx->shape.width / 32;  // partial columns per pair tile
+  const int resident = resident_ctas(ctx->shape);
+  const int tiles_per_cta = scan_tiles_per_cta(ctx->shape);
+  // accumulators: double sum, float min, max, mean per site
+  rc = ensure_buffer(reinterpret_cast<char**>(&ctx->acc), &ctx->acc_bytes, (size_t)S * 20);
+  if (rc) return rc;
+  double* acc_sum = static_cast<double*>(ctx->acc);
+  float* acc_min = reinterpret_cast<float*>(acc_sum + S);
+  float* acc_max = acc_min + S;
+  float* d_mean = acc_max + S;
+  // pair chunk: partials (3 x S x columns floats) within ~40% of the budget
+  const size_t budget = (size_t)(0.7 * (double)free_device_bytes()) + ctx->pool_bytes +
+                        ctx->stage_bytes;
+  const size_t per_tile = (size_t)3 * S * warps * sizeof(float);
+  int64_t chunk_tiles = std::max<int64_t>(1, (int64_t)(0.4 * (double)budget / (double)per_tile));
+  chunk_tiles = std::min<int64_t>(chunk_tiles, ceil_div(n_pairs, tile));
+  const int64_t chunk = chunk_tiles * tile;
+  const int64_t cols = chunk_tiles * warps;
+  rc = ensure_buffer(&ctx->stage, &ctx->stage_bytes, (size_t)3 * S * cols * sizeof(float));
+  if (rc) return rc;
+  float* p_sum = ctx->stage;
+  float* p_min = p_sum + (size_t)S * cols;
+  float* p_max = p_min + (size_t)S * cols;
+  const int busy = (int)std::min<int64_t>(
+      resident, ceil_div((int64_t)blocks.size() * chunk_tiles, tiles_per_cta));
+  const size_t slot = cta_slot_bytes(ctx->shape, core);
+  const size_t pool_budget = budget > (size_t)3 * S * cols * 4 ? budget - (size_t)3 * S * cols * 4 : slot;
+  int grid = 0;
+  rc = size_pool(ctx, core, busy, pool_budget, &grid);
+  if (rc) return rc;
+  const int32_t* d_pi = ctx->pairs;
+  const int32_t* d_pj = ctx->pairs + ctx->pairs_cap;
+  int which = 0;
+  for (int64_t off = 0; off < n_pairs; off += chunk, which ^= 1) {
+    const int64_t n = std::min(chunk, n_pairs - off);
+    std::vector<Task> tasks;
+    for (const Block& b : blocks) {
+      WindowOut wo{{p_sum, p_min, p_max, nullptr, nullptr}, 0, cols, 0};
+      const size_t first = tasks.size();
+      add_window_tasks(b, d_pi + off, d_pj + off, n, tile, wo, 0, kTaskSummary, 2.0f * ctx->ne,
+                       &tasks);
+      // a tile's partials go to its own columns: warps x tile index
+      for (size_t i = first; i < tasks.size(); ++i) tasks[i].out_off = (int64_t)(i - first) * warps;
+    }
+    rc = launch_tasks(ctx, tasks, which, core, grid, ctx->stream);
+    if (rc) return rc;
+    // a last, partial chunk fills only its own tiles' columns of each row
+    const int64_t used_cols = ceil_div(n, tile) * warps;
+    CUDA_TRY(launch_summary_fold(p_sum, p_min, p_max, S, used_cols, cols, acc_sum, acc_min,
+                                 acc_max, off == 0, ctx->stream));
+  }
+  CUDA_TRY(launch_summary_finish(acc_sum, S, (double)n_pairs, d_mean, ctx->stream));
+  CUDA_TRY(cudaMemcpyAsync(site_mean, d_mean, S * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaMemcpyAsync(site_min, acc_min, S * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaMemcpyAsync(site_max, acc_max, S * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return GSMC_OK;
+}
+
 int gsmc_run_fb_window(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j,
                        int64_t n_pairs, int64_t site_begin, int64_t site_end, int flags,
                        float* mean, float* lower, float* upper, float* alpha, float* beta) {
@@ -756,6 +839,35 @@ int gsmc_run_fb_blockwise_device(gsmc_ctx* ctx, const int32_t* d_pair_i, const i
                          (flags & GSMC_POSTERIOR) ? d_beta : nullptr};
   return run_direct(ctx, d_pair_i, d_pair_j, n_pairs, blocks, flags, out, ld_out, out_col0,
                     static_cast<cudaStream_t>(stream));
+}
+
+int gsmc_copy_to_host(int64_t n, void* const* dst, const void* const* src, const uint64_t* bytes,
+                      void* stream) {
+  if (n < 0 || (n > 0 && (!dst || !src || !bytes))) return fail(GSMC_E_INVALID, "bad copy list");
+  if (n == 0) return GSMC_OK;
+  HostCopier* copier = HostCopier::for_current_device();
+  if (!copier) return fail(GSMC_E_CUDA, "CUDA error: no device for the host copier");
+  cudaEvent_t ready = nullptr;
+  CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+  cudaError_t e = cudaEventRecord(ready, static_cast<cudaStream_t>(stream));
+  int first = (int)e;
+  for (int64_t i = 0; i < n && first == cudaSuccess; ++i) {
+    if (bytes[i] == 0) continue;
+    if (!dst[i] || !src[i]) {
+      first = -1;
+      break;
+    }
+    first = copier->enqueue(dst[i], (size_t)bytes[i], src[i], (size_t)bytes[i], (size_t)bytes[i], 1,
+                            ready);
+  }
+  const int drained = copier->drain();
+  cudaEventDestroy(ready);
+  if (first == -1) return fail(GSMC_E_INVALID, "null pointer in the copy list");
+  if (first != cudaSuccess)
+    return fail(GSMC_E_CUDA, "CUDA error: %s (device to host copy)", cudaGetErrorString((cudaError_t)first));
+  if (drained != cudaSuccess)
+    return fail(GSMC_E_CUDA, "CUDA error: %s (device to host copy)", cudaGetErrorString((cudaError_t)drained));
+  return GSMC_OK;
 }
 
 int gsmc_bitpack(const uint8_t* G, int64_t n_haps, int64_t n_sites, uint64_t* packed) {

@@ -36,7 +36,7 @@ namespace {
 #define GSMC_MIN_CTAS 6
 #endif
 
-template <int NP, int WIDTH>
+template <int NP, int WIDTH, bool SUMMARY>
 __global__ void __launch_bounds__(kThreads, NP == 1 ? GSMC_MIN_CTAS : GSMC_MIN_CTAS / 2)
     fb_scan_persistent(const ScanArgs a) {
   // The task descriptor lives in shared memory: its fields are uniform across
@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(kThreads, NP == 1 ? GSMC_MIN_CTAS : GSMC_MIN_C
       }
       __syncthreads();
       if (task_id < 0) break;
-      scan_task<NP, kThreads>(a, task, slot);
+      scan_task<NP, kThreads, SUMMARY>(a, task, slot);
     }
   } else {
     // each warp takes its own tasks
@@ -79,9 +79,48 @@ __global__ void __launch_bounds__(kThreads, NP == 1 ? GSMC_MIN_CTAS : GSMC_MIN_C
       int* dst = reinterpret_cast<int*>(&task[w]);
       if (lane < (int)(sizeof(Task) / 4)) dst[lane] = src[lane];
       __syncwarp();
-      scan_task<NP, 32>(a, task[w], slot);
+      scan_task<NP, 32, SUMMARY>(a, task[w], slot);
     }
   }
+}
+
+// One warp per site row: fold the row's per-warp partials into the site's
+// accumulators.  Lane l sums columns l, l + 32, ... in order, then a fixed
+// shuffle tree combines the lanes, so the result does not depend on timing.
+__global__ void summary_fold_kernel(const float* __restrict__ p_sum,
+                                    const float* __restrict__ p_min,
+                                    const float* __restrict__ p_max, int64_t rows, int64_t cols,
+                                    int64_t ld, double* __restrict__ acc_sum,
+                                    float* __restrict__ acc_min,
+                                    float* __restrict__ acc_max, bool first) {
+  const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= rows) return;  // whole warps leave together
+  const int64_t base = row * ld;
+  double sum = 0.0;
+  float mn = __int_as_float(0x7f800000), mx = -__int_as_float(0x7f800000);
+  for (int64_t c = lane; c < cols; c += 32) {
+    sum += (double)p_sum[base + c];
+    mn = fminf(mn, p_min[base + c]);
+    mx = fmaxf(mx, p_max[base + c]);
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    sum += __shfl_xor_sync(0xffffffffu, sum, d);
+    mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, d));
+    mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, d));
+  }
+  if (lane == 0) {
+    acc_sum[row] = first ? sum : acc_sum[row] + sum;
+    acc_min[row] = first ? mn : fminf(acc_min[row], mn);
+    acc_max[row] = first ? mx : fmaxf(acc_max[row], mx);
+  }
+}
+
+__global__ void summary_finish_kernel(const double* __restrict__ acc_sum, int64_t rows,
+                                      double n_pairs, float* __restrict__ site_mean) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < rows) site_mean[s] = (float)(acc_sum[s] / n_pairs);
 }
 
 // Pack genotypes: thread (h, word) builds 64 sites of haplotype h.
@@ -130,10 +169,25 @@ namespace {
 template <int NP, int WIDTH>
 int resident_of() {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fb_scan_persistent<NP, WIDTH>,
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fb_scan_persistent<NP, WIDTH, false>,
                                                     kThreads, 0) != cudaSuccess)
     return 0;
   return per_sm;
+}
+
+template <bool SUMMARY>
+void launch_shape(const ScanArgs& args, int grid, ScanShape shape, cudaStream_t stream) {
+  if (shape.width == 32) {
+    if (shape.pairs_per_thread == 2)
+      fb_scan_persistent<2, 32, SUMMARY><<<grid, kThreads, 0, stream>>>(args);
+    else
+      fb_scan_persistent<1, 32, SUMMARY><<<grid, kThreads, 0, stream>>>(args);
+  } else {
+    if (shape.pairs_per_thread == 2)
+      fb_scan_persistent<2, kThreads, SUMMARY><<<grid, kThreads, 0, stream>>>(args);
+    else
+      fb_scan_persistent<1, kThreads, SUMMARY><<<grid, kThreads, 0, stream>>>(args);
+  }
 }
 
 }  // namespace
@@ -151,20 +205,32 @@ int scan_resident_ctas(ScanShape shape) {
   return sms * per_sm;
 }
 
-cudaError_t launch_scan(const ScanArgs& args, int grid, ScanShape shape, cudaStream_t stream) {
+cudaError_t launch_scan(const ScanArgs& args, int grid, ScanShape shape, cudaStream_t stream,
+                        bool summary) {
   if (grid <= 0) return cudaSuccess;
   if (!scan_shape_valid(shape)) return cudaErrorInvalidValue;
-  if (shape.width == 32) {
-    if (shape.pairs_per_thread == 2)
-      fb_scan_persistent<2, 32><<<grid, kThreads, 0, stream>>>(args);
-    else
-      fb_scan_persistent<1, 32><<<grid, kThreads, 0, stream>>>(args);
-  } else {
-    if (shape.pairs_per_thread == 2)
-      fb_scan_persistent<2, kThreads><<<grid, kThreads, 0, stream>>>(args);
-    else
-      fb_scan_persistent<1, kThreads><<<grid, kThreads, 0, stream>>>(args);
-  }
+  if (summary)
+    launch_shape<true>(args, grid, shape, stream);
+  else
+    launch_shape<false>(args, grid, shape, stream);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_summary_fold(const float* p_sum, const float* p_min, const float* p_max,
+                                int64_t rows, int64_t cols, int64_t ld, double* acc_sum,
+                                float* acc_min, float* acc_max, bool first, cudaStream_t stream) {
+  if (rows <= 0 || cols <= 0) return cudaSuccess;
+  const int64_t threads = rows * 32;
+  summary_fold_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, stream>>>(
+      p_sum, p_min, p_max, rows, cols, ld, acc_sum, acc_min, acc_max, first);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_summary_finish(const double* acc_sum, int64_t rows, double n_pairs,
+                                  float* site_mean, cudaStream_t stream) {
+  if (rows <= 0) return cudaSuccess;
+  summary_finish_kernel<<<(unsigned)((rows + 255) / 256), 256, 0, stream>>>(acc_sum, rows, n_pairs,
+                                                                           site_mean);
   return cudaGetLastError();
 }
 

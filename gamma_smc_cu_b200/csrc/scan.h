@@ -17,8 +17,11 @@ struct SiteCode {
 // Zero entries stored before site 0 and after the last site of the code array.
 constexpr int kCodePad = 2;
 
-// Output selection of a task.
-enum TaskFlags { kTaskCI = 1, kTaskPosterior = 2 };
+// Output selection of a task.  kTaskSummary replaces the per-pair outputs by
+// per-warp partial reductions over the task's pairs at each core site: the
+// sum, minimum and maximum of the posterior means go to out[0], out[1] and
+// out[2] at (s - out_row0) * ldo + out_off + (warp within the tile).
+enum TaskFlags { kTaskCI = 1, kTaskPosterior = 2, kTaskSummary = 4 };
 
 // One unit of scan work: up to (tile width x pairs per thread) pairs over one
 // padded window.  Forward over [ps, ce), backward over [pe-1 .. cs], posterior
@@ -85,7 +88,20 @@ int scan_resident_ctas(ScanShape shape);
 // Launch the persistent scan over the task list of args with `grid`
 // CTAs; CTA b's tile t owns forward-state slot b * tiles_per_cta + t of
 // slot_rows x tile pairs float2.
-cudaError_t launch_scan(const ScanArgs& args, int grid, ScanShape shape, cudaStream_t stream);
+// slot_rows x tile pairs float2.  `summary`: every task is a kTaskSummary task.
+cudaError_t launch_scan(const ScanArgs& args, int grid, ScanShape shape, cudaStream_t stream,
+                        bool summary = false);
+
+// Fold per-warp partials (sum, min, max) of a summary launch -- rows x cols,
+// row pitch ld -- into per-site accumulators acc_sum (float64), acc_min,
+// acc_max [rows], in a fixed order (deterministic); `first` overwrites
+// instead of accumulating.
+cudaError_t launch_summary_fold(const float* p_sum, const float* p_min, const float* p_max,
+                                int64_t rows, int64_t cols, int64_t ld, double* acc_sum,
+                                float* acc_min, float* acc_max, bool first, cudaStream_t stream);
+// site_mean[s] = acc_sum[s] / n_pairs rounded to float32.
+cudaError_t launch_summary_finish(const double* acc_sum, int64_t rows, double n_pairs,
+                                  float* site_mean, cudaStream_t stream);
 
 // Pack [n_haps x n_sites] uint8 genotypes.  scan_layout: word-major 128-site
 // groups for the scan; otherwise the reference's row-major uint64 words.

@@ -102,17 +102,25 @@ __device__ __forceinline__ uint64_t word_at(const ulonglong2* g, int64_t nh, int
   return (s & 64) ? v.y : v.x;
 }
 
-// Posterior combine at one core site: forward state f, backward state (m, c)
-// (src/kernels/gamma_smc_flow.cu:708-734).
-__device__ __forceinline__ void combine_store(const Task& t, int64_t o, float2 f, float m, float c,
-                                              bool ci, bool post) {
+// Posterior at one core site: forward state f, backward state (m, c) ->
+// alpha, beta and the mean in generations (src/kernels/gamma_smc_flow.cu:708-722).
+__device__ __forceinline__ float posterior(float2 f, float m, float c, float unscale, float& a_s,
+                                           float& b_s) {
   const float ab = -2.0f * c;
   const float ba = pow10_bits(ab), bb = pow10_bits(__fsub_rn(ab, m));
   const float af = -2.0f * f.y;
   const float fa = pow10_bits(af), fb = pow10_bits(__fsub_rn(af, f.x));
-  const float a_s = __fsub_rn(__fadd_rn(fa, ba), 1.0f);
-  const float b_s = __fsub_rn(__fadd_rn(fb, bb), 1.0f);
-  const float mg = __fmul_rn(__fdiv_rn(a_s, fmaxf(b_s, 1e-10f)), t.unscale);
+  a_s = __fsub_rn(__fadd_rn(fa, ba), 1.0f);
+  b_s = __fsub_rn(__fadd_rn(fb, bb), 1.0f);
+  return __fmul_rn(__fdiv_rn(a_s, fmaxf(b_s, 1e-10f)), unscale);
+}
+
+// Posterior combine at one core site, stored per pair
+// (src/kernels/gamma_smc_flow.cu:708-734).
+__device__ __forceinline__ void combine_store(const Task& t, int64_t o, float2 f, float m, float c,
+                                              bool ci, bool post) {
+  float a_s, b_s;
+  const float mg = posterior(f, m, c, t.unscale, a_s, b_s);
   __stcs(t.out[0] + o, mg);
   if (ci) {
     // Wilson-Hilferty 95% bounds (src/kernels/gamma_smc_flow.cu:724-733).
@@ -140,15 +148,21 @@ constexpr int kThreads = 128;
 // One task: this thread's NP pairs over the task's padded window.  WIDTH
 // threads (a warp or the whole CTA) share the task; the forward states live in
 // the tile's slot, rows of WIDTH * NP pairs.
-template <int NP, int WIDTH>
+// SUMMARY selects the per-warp reductions of kTaskSummary tasks (a separate
+// instantiation, so the per-pair kernels carry none of its registers).
+template <int NP, int WIDTH, bool SUMMARY = false>
 __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, float2* slot) {
   static_assert(WIDTH == 32 || WIDTH == kThreads, "a task is run by one warp or one CTA");
   constexpr int kRow = WIDTH * NP;
   const int64_t nh = a.n_haps;
   const int ps = t.ps, cs = t.cs, ce = t.ce, pe = t.pe;
   const bool ci = (t.flags & kTaskCI) != 0, post = (t.flags & kTaskPosterior) != 0;
+  constexpr bool summary = SUMMARY;
   const int j0 = threadIdx.x & (WIDTH - 1);
-  if (j0 >= t.pair_count) return;
+  // Warps with no pair leave; lanes past the last pair of a partly filled warp
+  // walk along on pair (0, 0) with nothing stored (summary reductions need
+  // every lane of the warp).
+  if ((j0 & ~31) >= t.pair_count) return;
 
   const ulonglong2* gi[NP];
   const ulonglong2* gj[NP];
@@ -326,9 +340,37 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     Fetch fe[NP];
     const bool more = s > cs;
     if (more) bwd_fetch(s, sc, nx.layer, fe);
+    if constexpr (summary) {
+      // sum / min / max of the posterior means over the warp's live pairs,
+      // in a fixed shuffle order; lane 0 stores the warp's partials
+      float vs = 0.0f, vmin = __int_as_float(0x7f800000), vmax = -__int_as_float(0x7f800000);
 #pragma unroll
-    for (int k = 0; k < NP; ++k)
-      if (live[k]) combine_store(t, o + k * WIDTH, f[k], mb[k], cb[k], ci, post);
+      for (int k = 0; k < NP; ++k) {
+        float a_s, b_s;
+        const float mg = posterior(f[k], mb[k], cb[k], t.unscale, a_s, b_s);
+        if (live[k]) {
+          vs = __fadd_rn(vs, mg);
+          vmin = fminf(vmin, mg);
+          vmax = fmaxf(vmax, mg);
+        }
+      }
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) {
+        vs = __fadd_rn(vs, __shfl_xor_sync(0xffffffffu, vs, d));
+        vmin = fminf(vmin, __shfl_xor_sync(0xffffffffu, vmin, d));
+        vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, d));
+      }
+      if ((threadIdx.x & 31) == 0) {
+        const int64_t po = t.out_off + (int64_t)(s - t.out_row0) * t.ldo + (j0 >> 5);
+        t.out[0][po] = vs;
+        t.out[1][po] = vmin;
+        t.out[2][po] = vmax;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < NP; ++k)
+        if (live[k]) combine_store(t, o + k * WIDTH, f[k], mb[k], cb[k], ci, post);
+    }
     o -= t.ldo;
     if (more) bwd_finish(sc, fe);
     cur = nx;

@@ -26,6 +26,7 @@ from __future__ import annotations
 import collections
 import threading
 import time
+import weakref
 from concurrent.futures import Future
 
 import numpy as np
@@ -45,10 +46,76 @@ def _free_device_bytes(device):
     return torch.cuda.mem_get_info(device)[0]
 
 
+def _new_arena(nbytes):
+    return PinnedArena(nbytes)
+
+
 def _bind_thread(device):
     import torch
     if torch.cuda.is_available():
         torch.cuda.set_device(device)
+
+
+class _Region:
+    """Owner of one arena region; numpy views of it keep it alive, and the
+    region returns to the arena when the last view is garbage-collected."""
+
+    def __init__(self, arena, offset, nbytes):
+        self.__array_interface__ = {"shape": (nbytes // BYTES_PER_FLOAT,), "typestr": "<f4",
+                                    "data": (arena.base + offset, False), "version": 3}
+        weakref.finalize(self, arena.release, offset, nbytes)
+
+
+class PinnedArena:
+    """First-fit allocator over one pinned host buffer that results are
+    copied into; hands out float32 views (see _Region)."""
+
+    ALIGN = 256
+
+    def __init__(self, nbytes):
+        import torch
+        self.size = int(nbytes)
+        self._t = torch.empty(max(self.size, 1), dtype=torch.uint8, pin_memory=True)
+        self.base = self._t.data_ptr()
+        self._free = [(0, self.size)]   # sorted (offset, length)
+        self._lock = threading.Lock()
+        self.in_use = 0
+
+    def alloc(self, nbytes):
+        """A float32 view of nbytes (rounded up), or None if nothing fits."""
+        n = -(-max(int(nbytes), 1) // self.ALIGN) * self.ALIGN
+        with self._lock:
+            for i, (off, ln) in enumerate(self._free):
+                if ln >= n:
+                    if ln == n:
+                        del self._free[i]
+                    else:
+                        self._free[i] = (off + n, ln - n)
+                    self.in_use += n
+                    break
+            else:
+                return None
+        return np.asarray(_Region(self, off, n))
+
+    def release(self, off, n):
+        with self._lock:
+            self.in_use -= n
+            self._free.append((off, n))
+            self._free.sort()
+            merged = []
+            for o, ln in self._free:
+                if merged and merged[-1][0] + merged[-1][1] == o:
+                    merged[-1] = (merged[-1][0], merged[-1][1] + ln)
+                else:
+                    merged.append((o, ln))
+            self._free = merged
+
+
+def _pinned_floats(n):
+    """A pinned float32 array of n elements outside the arena (torch's
+    caching host allocator)."""
+    import torch
+    return torch.empty(max(int(n), 1), dtype=torch.float32, pin_memory=True).numpy()
 
 
 class _Request:
@@ -89,7 +156,7 @@ class TmrcaServer:
     def __init__(self, ctx, positions=None, max_inflight=3, core_block_sites=4096,
                  flank_sites=2048, tile_width=128, pairs_per_thread=1, use_graph=True,
                  hbm_budget=None, max_tasks=1 << 15, max_batch_requests=4096,
-                 poll_interval=50e-6):
+                 max_batch_pair_sites=1 << 29, pinned_bytes=1 << 30, poll_interval=50e-6):
         self.ctx = ctx
         self.positions = None if positions is None else np.asarray(positions, np.float64)
         self.device = ctx.device_id
@@ -107,6 +174,8 @@ class TmrcaServer:
         self.hbm_budget = int(hbm_budget)
         self.max_tasks = int(max_tasks)
         self.max_batch_requests = int(max_batch_requests)
+        self.max_batch_pair_sites = float(max_batch_pair_sites)
+        self.arena = _new_arena(pinned_bytes) if pinned_bytes else None
         self.poll_interval = float(poll_interval)
         self._pending = collections.deque()
         self._cv = threading.Condition()
@@ -175,14 +244,19 @@ class TmrcaServer:
                 self.counters.clear()
         out = {"completed": len(done), **counters}
         if done:
-            lat = np.array([r.t_done - r.t_arrive for r in done]) * 1e3
-            queue = np.array([r.t_admit - r.t_arrive for r in done]) * 1e3
-            span = max(r.t_done for r in done) - min(r.t_arrive for r in done)
-            ps = float(sum(r.job.pair_sites for r in done))
+            t = np.array(done)
+            lat = (t[:, 2] - t[:, 0]) * 1e3
+            queue = (t[:, 1] - t[:, 0]) * 1e3
+            service = (t[:, 2] - t[:, 1]) * 1e3
+            span = float(t[:, 2].max() - t[:, 0].min())
+            ps = float(t[:, 3].sum())
             out.update({"p50_ms": float(np.percentile(lat, 50)),
                         "p99_ms": float(np.percentile(lat, 99)),
                         "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
                         "queue_p50_ms": float(np.percentile(queue, 50)),
+                        "queue_p99_ms": float(np.percentile(queue, 99)),
+                        "service_p50_ms": float(np.percentile(service, 50)),
+                        "service_p99_ms": float(np.percentile(service, 99)),
                         "pair_sites": ps, "span_s": span,
                         "pair_sites_per_s": ps / span if span > 0 else None})
         return out
@@ -190,15 +264,19 @@ class TmrcaServer:
     # ------------------------------------------------------------- scheduler
 
     def _finish(self, slot):
-        results = slot.batch.layout.results(slot.batch.h_out.numpy())
+        # views into the batch's pinned host buffer: an arena region returns
+        # to the arena once the caller drops the last result array using it
+        results = slot.batch.layout.results(slot.batch.h_out)
         now = time.perf_counter()
         for req, res in zip(slot.requests, results):
             req.t_done = now
-            # copy out of the pinned buffer so it can be reused
-            req.future.set_result({k: np.array(v) for k, v in res.items()})
+            req.future.set_result(res)
         with self._cv:
             self._in_use -= slot.bytes
-            self._done.extend(slot.requests)
+            # timings only: the requests (and the results their futures hold)
+            # are not kept, so result memory returns once the caller drops it
+            self._done.extend((r.t_arrive, r.t_admit, r.t_done, float(r.job.pair_sites))
+                              for r in slot.requests)
             self.counters["batches"] += 1
         slot.batch = None
         slot.requests = []
@@ -206,7 +284,7 @@ class TmrcaServer:
 
     def _admit(self, slot):
         """Move the waiting queries that fit into a new batch on ``slot``."""
-        take, nbytes, ntasks = [], 0, 0
+        take, nbytes, ntasks, work = [], 0, 0, 0.0
         with self._cv:
             while self._pending and len(take) < self.max_batch_requests:
                 req = self._pending[0]
@@ -218,13 +296,17 @@ class TmrcaServer:
                         f"server holds at most {self.hbm_budget} bytes and {self.max_tasks} "
                         "tasks per batch"))
                     continue
-                if (self._in_use + nbytes + req.bytes > self.hbm_budget
-                        or ntasks + req.tasks > self.max_tasks):
+                if take and (self._in_use + nbytes + req.bytes > self.hbm_budget
+                             or ntasks + req.tasks > self.max_tasks
+                             or work + req.job.pair_sites > self.max_batch_pair_sites):
+                    break
+                if self._in_use + req.bytes > self.hbm_budget:
                     break
                 self._pending.popleft()
                 take.append(req)
                 nbytes += req.bytes
                 ntasks += req.tasks
+                work += req.job.pair_sites
             if not take:
                 return False
             self._in_use += nbytes
@@ -233,8 +315,14 @@ class TmrcaServer:
         for r in take:
             r.t_admit = now
         try:
-            batch = DeviceBatch(Layout([r.job for r in take]), self.device)
-            batch.launch(slot.executor, slot.stream)
+            layout = Layout([r.job for r in take])
+            host = self.arena.alloc(layout.out_floats * BYTES_PER_FLOAT) if self.arena else None
+            if host is None:
+                host = _pinned_floats(layout.out_floats)
+                with self._cv:
+                    self.counters["outside_arena"] += 1
+            batch = DeviceBatch(layout, self.device)
+            batch.launch(slot.executor, slot.stream, host=host)
         except Exception as e:  # a launch failure fails the batch's queries
             with self._cv:
                 self._in_use -= nbytes

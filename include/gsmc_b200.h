@@ -223,6 +223,18 @@ int gsmc_exec_timing(gsmc_exec* exec, int enable);
 int gsmc_exec_timing_read(gsmc_exec* exec, double* kernel_ms, int64_t* launches,
                           double* pair_sites);
 
+/*
+ * Copy n device regions (src[i], bytes[i]) into host memory dst[i] -- pageable
+ * or pinned -- once the work already enqueued on `stream` has finished;
+ * returns when every byte has landed.  Data moves through the library's
+ * pinned ring with parallel host threads, so large pageable results need no
+ * pinning.  For collecting the outputs of gsmc_exec_run; no reference
+ * counterpart (the reference copied with blocking cudaMemcpy,
+ * src/bindings.cpp:2965-2975).
+ */
+int gsmc_copy_to_host(int64_t n, void* const* dst, const void* const* src,
+                      const uint64_t* bytes, void* stream);
+
 /* Bytes of device scratch the context currently holds (forward-state pool). */
 int gsmc_ctx_scratch_bytes(const gsmc_ctx* ctx, uint64_t* bytes);
 

@@ -43,9 +43,11 @@ def test_layout_packs_pairs_and_outputs():
     lay.pack_pairs(pairs)
     assert pairs.tolist() == [1, 2, 2, 0, 0, 1, 3, 2]
     # outputs: job 0 mean (15 -> 64 floats), job 1 mean/lower/upper (2 each -> 64 each)
-    assert lay.out_off[0] == [0, None, None, None, None]
-    assert lay.out_off[1] == [64, 128, 192, None, None]
-    assert lay.out_off[2] == [256, None, None, 256, 256]
+    assert lay.out_off[0].tolist() == [0, -1, -1, -1, -1]
+    assert lay.out_off[1].tolist() == [64, 128, 192, -1, -1]
+    assert lay.out_off[2].tolist() == [256, -1, -1, 256, 256]
+    assert [r[:2] for r in lay.regions()] == [(0, "mean"), (1, "mean"), (1, "lower"),
+                                              (1, "upper")]
     arr = lay.c_jobs(1000, 50000)
     assert arr[1].pair_i == 1000 + 4 * 6 and arr[1].pair_j == 1000 + 4 * 7
     assert arr[1].out[0] == 50000 + 4 * 64 and arr[1].out[3] is None

@@ -114,7 +114,7 @@ def test_executor_reuse_and_two_streams(small_ctx, oracle):
             b.launch(e, st)
             batches.append(b)
     for b in batches:
-        for j, r in zip(b.layout.jobs, b.results()):
+        for j, r in zip(b.layout.jobs, b.to_host()):
             want = _oracle_window(oracle, packed, pos, tables, j.pairs, j.site_begin,
                                   j.site_end, j.mean_only, j.return_posterior)
             _check(r, want)

@@ -10,6 +10,18 @@ import pytest
 from gamma_smc_cu_b200 import serve
 
 
+class NumpyArena(serve.PinnedArena):
+    """The arena's allocator over ordinary host memory."""
+
+    def __init__(self, nbytes):
+        self.size = int(nbytes)
+        self._buf = np.zeros(max(self.size, 1), np.uint8)
+        self.base = self._buf.ctypes.data
+        self._free = [(0, self.size)]
+        self._lock = threading.Lock()
+        self.in_use = 0
+
+
 class FakeCtx:
     n_haps = 20
     n_sites = 500
@@ -61,20 +73,20 @@ def make_batch_cls(rec, server_ref):
             self.layout = layout
             self.done = None
 
-        def launch(self, executor, stream):
+        def launch(self, executor, stream, host=None):
             for j in self.layout.jobs:
                 if rec.fail_tag is not None and j.pairs.size and j.pairs[0, 0] == rec.fail_tag:
                     raise RuntimeError("injected launch failure")
-            out = np.zeros(self.layout.out_floats, np.float32)
+            out = host
             for j, offs in zip(self.layout.jobs, self.layout.out_off):
                 for o in offs:
-                    if o is not None:
+                    if o >= 0:
                         # value = site index + 1000 * first pair's i
                         v = (np.arange(j.site_begin, j.site_end)[:, None]
                              + 1000.0 * (j.pairs[0, 0] if j.n_pairs else 0))
                         out[o:o + j.rows * j.n_pairs] = np.broadcast_to(
                             v, (j.rows, j.n_pairs)).ravel()
-            self.h_out = _Host(out)
+            self.h_out = out
             with rec.lock:
                 busy = sum(1 for s in server_ref[0].slots if s.batch is not None)
                 rec.overlaps += busy > 0
@@ -97,6 +109,8 @@ def server_factory(monkeypatch):
         monkeypatch.setattr(serve, "_new_stream", lambda d: object())
         monkeypatch.setattr(serve, "_free_device_bytes", lambda d: 1 << 30)
         monkeypatch.setattr(serve, "_bind_thread", lambda d: None)
+        monkeypatch.setattr(serve, "_new_arena", NumpyArena)
+        monkeypatch.setattr(serve, "_pinned_floats", lambda n: np.zeros(max(n, 1), np.float32))
         positions = np.arange(500, dtype=np.float64) * 10.0
         s = serve.TmrcaServer(FakeCtx(), positions=positions, **kw)
         ref[0] = s
@@ -193,3 +207,32 @@ def test_submit_validation_and_regions(server_factory):
     s.close()
     with pytest.raises(RuntimeError, match="closed"):
         s.submit([(1, 0)], 0, 5)
+
+
+def test_arena_views_return_memory_when_dropped():
+    import gc
+    a = NumpyArena(4096)
+    v1 = a.alloc(1000)           # 1024 bytes
+    v2 = a.alloc(2000)           # 2048 bytes
+    assert v1.dtype == np.float32 and v1.size == 256 and v2.size == 512
+    assert a.alloc(2048) is None and a.in_use == 3072
+    part = v1[10:20].reshape(2, 5)   # a view keeps the region alive
+    v1[:] = 1.0
+    del v1
+    gc.collect()
+    assert a.in_use == 3072 and part.sum() == 10.0
+    del part, v2
+    gc.collect()
+    assert a.in_use == 0 and a._free == [(0, 4096)]
+    assert a.alloc(4096).size == 1024
+
+
+def test_results_outlive_arena_pressure(server_factory):
+    """Callers that keep results do not stall the server: batches that no
+    longer fit the arena get their own pinned buffer."""
+    s, rec = server_factory(max_inflight=2, pinned_bytes=8192)
+    kept = [s.submit([(i, 0), (i, 1)], 0, 400) for i in range(1, 8)]   # 3.2 kB each
+    res = [f.result(timeout=10) for f in kept]
+    for i, r in enumerate(res, start=1):
+        assert np.array_equal(r["mean"][:, 1], np.arange(400) + 1000.0 * i)
+    assert s.stats()["outside_arena"] >= 1

@@ -185,6 +185,44 @@ class FlowContext:
                                              *self._out_ptrs(out)))
         return out
 
+    def run_fwd(self, pairs, mean_only=True):
+        """Forward-only (filtered) posterior, the reference's ``run_fwd``:
+        dict with ``mean`` (and ``lower``/``upper`` unless mean_only) of shape
+        [n_sites, n_pairs] float32."""
+        pi, pj = _split_pairs(pairs)
+        P = len(pi)
+        if P == 0:
+            return {"mean": np.empty((self._S, 0), np.float32)}
+        out = {"mean": np.empty((self._S, P), np.float32)}
+        if not mean_only:
+            out["lower"] = np.empty((self._S, P), np.float32)
+            out["upper"] = np.empty((self._S, P), np.float32)
+        check(_lib.load().gsmc_run_fwd(self._h, ptr(pi, _lib.c_i32p), ptr(pj, _lib.c_i32p), P,
+                                       0 if mean_only else GSMC_CI,
+                                       ptr(out["mean"], _lib.c_f32p),
+                                       ptr(out.get("lower"), _lib.c_f32p),
+                                       ptr(out.get("upper"), _lib.c_f32p)))
+        return out
+
+    def run_fb_summary(self, pairs, core_block_sites=0, flank_sites=2048, pair_batch_size=-1):
+        """Per-site mean / min / max over the pairs of the posterior mean, with
+        no [n_sites, n_pairs] output (reference ``run_fb_summary``; the
+        reference's site_min/site_max are left unwritten there, here they are
+        the extremes over the pairs).  ``core_block_sites > 0`` decodes
+        blockwise.  Returns site_mean, site_min, site_max ([n_sites] float32)
+        and n_pairs."""
+        pi, pj = _split_pairs(pairs)
+        P = len(pi)
+        if P == 0:
+            return {"site_mean": np.zeros(0, np.float32)}
+        out = {k: np.empty(self._S, np.float32) for k in ("site_mean", "site_min", "site_max")}
+        check(_lib.load().gsmc_run_fb_summary(
+            self._h, ptr(pi, _lib.c_i32p), ptr(pj, _lib.c_i32p), P, int(core_block_sites),
+            int(flank_sites), int(pair_batch_size), ptr(out["site_mean"], _lib.c_f32p),
+            ptr(out["site_min"], _lib.c_f32p), ptr(out["site_max"], _lib.c_f32p)))
+        out["n_pairs"] = P
+        return out
+
     def run_fb_blockwise(self, pairs, core_block_sites=8192, flank_sites=2048,
                          pair_batch_size=256, max_streams=1, mean_only=True,
                          return_posterior=False):

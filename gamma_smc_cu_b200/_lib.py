@@ -100,6 +100,9 @@ SIGNATURES = {
                                       ctypes.POINTER(ctypes.c_double)]),
     "gsmc_copy_to_host": (c_int, [c_i64, ctypes.POINTER(c_vp), ctypes.POINTER(c_vp), c_u64p,
                                   c_vp]),
+    "gsmc_run_fb_summary": (c_int, [c_vp, c_i32p, c_i32p, c_i64, c_i64, c_i64, c_i64, c_f32p,
+                                    c_f32p, c_f32p]),
+    "gsmc_run_fwd": (c_int, [c_vp, c_i32p, c_i32p, c_i64, c_int, c_f32p, c_f32p, c_f32p]),
     "gsmc_ctx_scratch_bytes": (c_int, [c_vp, c_u64p]),
     "gsmc_ctx_timing": (c_int, [c_vp, c_int]),
     "gsmc_ctx_timing_read": (c_int, [c_vp, ctypes.POINTER(ctypes.c_double), c_i64p,

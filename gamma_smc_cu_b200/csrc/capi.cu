@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "ctx_view.h"
+#include "fwd.h"
 #include "gsmc_b200.h"
 #include "hostcopy.h"
 #include "scan.h"
@@ -54,6 +55,11 @@ struct TableSet {
   int L = 0;
   float4* site = nullptr;   // [4][L][2450][2]
   float4* chunk = nullptr;  // [2450][2]
+  // the hom multi-step table, kept on the host until the forward-only path
+  // first needs its half-precision patch copy (built on the device then)
+  std::vector<float> hom_m, hom_c;  // [L][2550]
+  uint4* hom_half = nullptr;        // [L][2450] half patches
+  std::mutex half_mu;
   int refs = 0;
 };
 
@@ -80,6 +86,10 @@ int acquire_tables(int device, const char* ff_path, float ne, float mu, float rh
   build_layers(ff, L, srho, smu, 0, &layers);
   std::vector<float> site, chunk;
   build_scan_layout(layers, &site, &chunk, 0);
+  auto keep_hom = [&](TableSet* t) {
+    t->hom_m = std::move(layers.t[kHomMean]);
+    t->hom_c = std::move(layers.t[kHomCv]);
+  };
   auto ts = std::make_unique<TableSet>();
   ts->device = device;
   ts->L = L;
@@ -91,6 +101,7 @@ int acquire_tables(int device, const char* ff_path, float ne, float mu, float rh
   CUDA_TRY(cudaMemcpy(ts->site, site.data(), site.size() * sizeof(float), cudaMemcpyHostToDevice));
   CUDA_TRY(cudaMemcpy(ts->chunk, chunk.data(), chunk.size() * sizeof(float),
                       cudaMemcpyHostToDevice));
+  keep_hom(ts.get());
   ts->refs = 1;
   *out = ts.get();
   g_tables[key] = ts.release();
@@ -111,6 +122,7 @@ void release_tables(TableSet* ts) {
   cudaSetDevice(ts->device);
   cudaFree(ts->site);
   cudaFree(ts->chunk);
+  cudaFree(ts->hom_half);
   cudaSetDevice(prev);
   delete ts;
 }
@@ -158,6 +170,8 @@ struct gsmc_ctx {
   size_t stage_bytes = 0;
   void* acc = nullptr;     // summary accumulators: double sum, float min, max, mean per site
   size_t acc_bytes = 0;
+  std::vector<double> positions;  // host copy, for the forward-only gap codes
+  FwdCode* fwd_code = nullptr;    // forward-only gap codes, built on first use
   unsigned char* tasks[2] = {nullptr, nullptr};  // task lists of alternating launches
   size_t tasks_cap[2] = {0, 0};                  // bytes
   cudaEvent_t stage_free[2] = {nullptr, nullptr};
@@ -573,6 +587,7 @@ int gsmc_ctx_create(const uint8_t* G, int64_t n_haps, int64_t n_sites, const dou
     const int chunks = (k - 1) / L;
     codes[s + kCodePad] = SiteCode{(k - chunks * L - 1) * kLayerF4, chunks};
   }
+  ctx->positions.assign(positions, positions + n_sites);
   SiteCode* code_base = nullptr;
   CUDA_TRY(cudaMalloc(&code_base, codes.size() * sizeof(SiteCode)));
   ctx->code = code_base + kCodePad;
@@ -599,6 +614,7 @@ int gsmc_ctx_destroy(gsmc_ctx* ctx) {
   cudaFree(ctx->pairs);
   cudaFree(ctx->stage);
   cudaFree(ctx->acc);
+  cudaFree(ctx->fwd_code);
   for (int i = 0; i < 2; ++i) {
     cudaFree(ctx->tasks[i]);
     if (ctx->stage_free[i]) cudaEventDestroy(ctx->stage_free[i]);
@@ -695,10 +711,13 @@ int gsmc_run_fb(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j, int
 
 int gsmc_run_fb_summary(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j,
                         int64_t n_pairs, int64_t core_block_sites, int64_t flank_sites,
-                        float* site_mean, float* site_min, float* site_max) {
+                        int64_t pair_batch_size, float* site_mean, float* site_min,
+                        float* site_max) {
   if (int rc = check_ctx(ctx)) return rc;
   if (n_pairs < 0) return fail(GSMC_E_INVALID, "negative pair count");
   if (flank_sites < 0) return fail(GSMC_E_INVALID, "flank_sites must be non-negative.");
+  if (pair_batch_size == 0 || pair_batch_size < -1)
+    return fail(GSMC_E_INVALID, "pair_batch_size must be positive or -1 for auto.");
   const int64_t S = ctx->n_sites;
   if (n_pairs == 0 || S == 0) return GSMC_OK;
   if (!pair_i || !pair_j) return fail(GSMC_E_INVALID, "null pair arrays");
@@ -729,6 +748,8 @@ int gsmc_run_fb_summary(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pai
   const size_t per_tile = (size_t)3 * S * warps * sizeof(float);
   int64_t chunk_tiles = std::max<int64_t>(1, (int64_t)(0.4 * (double)budget / (double)per_tile));
   chunk_tiles = std::min<int64_t>(chunk_tiles, ceil_div(n_pairs, tile));
+  if (pair_batch_size > 0)
+    chunk_tiles = std::min<int64_t>(chunk_tiles, std::max<int64_t>(1, pair_batch_size / tile));
   const int64_t chunk = chunk_tiles * tile;
   const int64_t cols = chunk_tiles * warps;
   rc = ensure_buffer(&ctx->stage, &ctx->stage_bytes, (size_t)3 * S * cols * sizeof(float));
@@ -759,8 +780,12 @@ int gsmc_run_fb_summary(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pai
     }
     rc = launch_tasks(ctx, tasks, which, core, grid, ctx->stream);
     if (rc) return rc;
-    // a last, partial chunk fills only its own tiles' columns of each row
-    const int64_t used_cols = ceil_div(n, tile) * warps;
+    // columns written: every warp of a full tile, and of the last tile the
+    // warps that hold a pair (warp w of a tile starts at pair 32 w; warps
+    // past the last pair leave without writing)
+    const int64_t rem = n % tile;
+    const int64_t used_cols = (n / tile) * warps +
+                              (rem ? ceil_div(std::min<int64_t>(rem, ctx->shape.width), 32) : 0);
     CUDA_TRY(launch_summary_fold(p_sum, p_min, p_max, S, used_cols, cols, acc_sum, acc_min,
                                  acc_max, off == 0, ctx->stream));
   }
@@ -769,6 +794,114 @@ int gsmc_run_fb_summary(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pai
   CUDA_TRY(cudaMemcpyAsync(site_min, acc_min, S * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_TRY(cudaMemcpyAsync(site_max, acc_max, S * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return GSMC_OK;
+}
+
+int gsmc_run_fwd(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j, int64_t n_pairs,
+                 int flags, float* mean, float* lower, float* upper) {
+  if (int rc = check_ctx(ctx)) return rc;
+  if (n_pairs < 0) return fail(GSMC_E_INVALID, "negative pair count");
+  const int64_t S = ctx->n_sites;
+  const bool ci = (flags & GSMC_CI) != 0;
+  if (n_pairs == 0 || S == 0) return GSMC_OK;
+  if (!pair_i || !pair_j || !mean || (ci && (!lower || !upper)))
+    return fail(GSMC_E_INVALID, "null pair or output array");
+  if (S > 0x7fffffff) return fail(GSMC_E_INVALID, "too many sites");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  int rc = upload_pairs(ctx, pair_i, pair_j, n_pairs);
+  if (rc) return rc;
+  TableSet* ts = ctx->tables;
+  const int L = ts->L;
+  {
+    // half patches of the hom table, once per table set
+    std::lock_guard<std::mutex> lock(ts->half_mu);
+    if (!ts->hom_half) {
+      std::vector<float> patches((size_t)L * kPatches * 8);
+      for (int k = 0; k < L; ++k)
+        pack_patches(ts->hom_m.data() + (size_t)k * kCells, ts->hom_c.data() + (size_t)k * kCells,
+                     patches.data() + (size_t)k * kPatches * 8);
+      float* tmp = nullptr;
+      CUDA_TRY(cudaMalloc(&tmp, patches.size() * sizeof(float)));
+      cudaError_t e = cudaMemcpy(tmp, patches.data(), patches.size() * sizeof(float),
+                                 cudaMemcpyHostToDevice);
+      uint4* half = nullptr;
+      if (e == cudaSuccess) e = cudaMalloc(&half, patches.size() * 2);
+      if (e == cudaSuccess) e = launch_to_half(tmp, half, patches.size(), ctx->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+      cudaFree(tmp);
+      if (e != cudaSuccess) {
+        cudaFree(half);
+        return fail(GSMC_E_CUDA, "CUDA error: %s (half table)", cudaGetErrorString(e));
+      }
+      ts->hom_half = half;
+    }
+  }
+  if (!ctx->fwd_code) {
+    // gap k = trunc(pos[s] - pos[s-1] + 0.5): `chunks` lookups in layer L-1,
+    // then layer k - chunks * L - 1; nothing at site 0 or for k <= 0
+    // (src/kernels/gamma_smc_flow.cu:1176-1188, 1225-1231)
+    std::vector<FwdCode> codes((size_t)S, FwdCode{-1, 0});
+    double prev = 0.0;
+    for (int64_t s2 = 0; s2 < S; ++s2) {
+      const double g = ctx->positions[s2] - prev + 0.5;
+      prev = ctx->positions[s2];
+      const int k = g >= 2147483647.0 ? 2147483647 : (int)g;
+      if (s2 == 0 || k <= 0) continue;
+      const int chunks = (k - 1) / L;
+      codes[s2] = FwdCode{k - chunks * L - 1, chunks};
+    }
+    CUDA_TRY(cudaMalloc(&ctx->fwd_code, codes.size() * sizeof(FwdCode)));
+    CUDA_TRY(cudaMemcpy(ctx->fwd_code, codes.data(), codes.size() * sizeof(FwdCode),
+                        cudaMemcpyHostToDevice));
+  }
+  // pair chunks whose outputs fit the stage; rows copied to the host arrays
+  const int nout = ci ? 3 : 1;
+  const size_t budget = (size_t)(0.5 * (double)free_device_bytes()) + ctx->stage_bytes;
+  int64_t chunk = std::max<int64_t>(1, (int64_t)(budget / ((size_t)S * nout * sizeof(float))));
+  chunk = std::min<int64_t>(chunk, n_pairs);
+  if (chunk < n_pairs) chunk = std::max<int64_t>(128, chunk / 128 * 128);
+  rc = ensure_buffer(&ctx->stage, &ctx->stage_bytes, (size_t)S * chunk * nout * sizeof(float));
+  if (rc) return rc;
+  HostCopier* copier = HostCopier::for_current_device();
+  if (!copier) return fail(GSMC_E_CUDA, "CUDA error: no device for the host copier");
+  cudaEvent_t done = nullptr;
+  CUDA_TRY(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+  int first = GSMC_OK;
+  float* host[3] = {mean, lower, upper};
+  for (int64_t off = 0; off < n_pairs && first == GSMC_OK; off += chunk) {
+    const int64_t n = std::min(chunk, n_pairs - off);
+    // the stage is rewritten only after the previous chunk's copies read it
+    int e = copier->drain();
+    FwdArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.geno = ctx->geno;
+    a.n_haps = ctx->n_haps;
+    a.code = ctx->fwd_code;
+    a.tab = ts->hom_half;
+    a.L = L;
+    a.n_sites = (int)S;
+    a.pi = ctx->pairs + off;
+    a.pj = ctx->pairs + ctx->pairs_cap + off;
+    a.n_pairs = (int)n;
+    a.two_ne = 2.0f * ctx->ne;
+    a.mean = ctx->stage;
+    a.lower = ci ? ctx->stage + (size_t)S * n : nullptr;
+    a.upper = ci ? ctx->stage + (size_t)2 * S * n : nullptr;
+    a.ldo = n;
+    if (e == cudaSuccess) e = launch_fwd_only(a, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(done, ctx->stream);
+    for (int k = 0; k < nout && e == cudaSuccess; ++k)
+      e = copier->enqueue(host[k] + off, (size_t)n_pairs * sizeof(float),
+                          ctx->stage + (size_t)k * S * n, (size_t)n * sizeof(float),
+                          (size_t)n * sizeof(float), (size_t)S, done);
+    if (e != cudaSuccess)
+      first = fail(GSMC_E_CUDA, "CUDA error: %s (forward-only)", cudaGetErrorString((cudaError_t)e));
+  }
+  const int e = copier->drain();
+  cudaEventDestroy(done);
+  if (first) return first;
+  if (e != cudaSuccess)
+    return fail(GSMC_E_CUDA, "CUDA error: %s (device to host copy)", cudaGetErrorString((cudaError_t)e));
   return GSMC_OK;
 }
 

@@ -1,0 +1,37 @@
+// Forward-only (filtered) posterior kernel: FlowContext.run_fwd.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gsmc {
+
+// Gap code of the forward-only path at one site: `chunks` lookups in the last
+// layer, then one in layer `layer` (-1: none -- site 0 and zero gaps).
+struct FwdCode {
+  int layer;
+  int chunks;
+};
+
+struct FwdArgs {
+  const ulonglong2* geno;  // scan genotype layout
+  int64_t n_haps;
+  const FwdCode* code;     // [n_sites]
+  const uint4* tab;        // [L][patches] half patches of the hom multi-step table
+  int L;
+  int n_sites;
+  const int32_t* pi;
+  const int32_t* pj;
+  int n_pairs;
+  float two_ne;
+  float* mean;             // [n_sites][ldo]
+  float* lower;            // null: no bounds
+  float* upper;
+  int64_t ldo;
+};
+
+cudaError_t launch_fwd_only(const FwdArgs& a, cudaStream_t stream);
+// n floats -> n halves (round to nearest even) on the device.
+cudaError_t launch_to_half(const float* src, void* dst, size_t n, cudaStream_t stream);
+
+}  // namespace gsmc

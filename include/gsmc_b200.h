@@ -107,6 +107,36 @@ int gsmc_run_fb_window(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair
                        int64_t n_pairs, int64_t site_begin, int64_t site_end, int flags,
                        float* mean, float* lower, float* upper, float* alpha, float* beta);
 
+/*
+ * Per-site summary over pairs without materialising [n_sites x n_pairs]:
+ * site_mean[s] = mean over the pairs of the posterior mean at site s, and
+ * site_min / site_max its extremes, into HOST arrays of n_sites float32.
+ * The scan reduces each warp's pairs in registers; partials are folded in a
+ * fixed order with a float64 sum, so results are deterministic.
+ * core_block_sites <= 0 decodes the full sequence (the reference's
+ * run_fb_summary); > 0 decodes blockwise with flank_sites.  pair_batch_size
+ * (-1 = auto) caps the pairs folded per pass.
+ * Replaces FlowContext::run_fb_summary (src/bindings.cpp:2695-2788) and
+ * gamma_smc_flow_cached_fb_reduce_gpu (src/kernels/gamma_smc_flow.cu:
+ * 1574-1683), whose float atomics are order-dependent and whose min/max
+ * outputs are never written.
+ */
+int gsmc_run_fb_summary(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j,
+                        int64_t n_pairs, int64_t core_block_sites, int64_t flank_sites,
+                        int64_t pair_batch_size, float* site_mean, float* site_min,
+                        float* site_max);
+
+/*
+ * Forward-only (filtered) posterior for n_pairs pairs into HOST arrays of
+ * [n_sites x n_pairs] float32: mean, and lower/upper when flags has GSMC_CI.
+ * Decoded as the reference's run_fwd: the hom multi-step table rounded to
+ * float16, a closed-form het emission, no backward pass.
+ * Replaces FlowContext::run_fwd (src/bindings.cpp:2794-2849) and
+ * gamma_smc_flow_h2_fwd_gpu (src/kernels/gamma_smc_flow.cu:1136-1295).
+ */
+int gsmc_run_fwd(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j, int64_t n_pairs,
+                 int flags, float* mean, float* lower, float* upper);
+
 /* Number of windows make_block_windows yields for (n_sites, core_block_sites). */
 int gsmc_block_count(int64_t n_sites, int64_t core_block_sites, int64_t* n_blocks);
 

@@ -12,6 +12,8 @@
 //   * cached FB kernels (full + block) src/kernels/gamma_smc_flow.cu:112-131,
 //     160-163, 408-514, 567-609, 632-669, 678-754, 762-839
 //   * bitpack                         src/kernels/bitpack.cu:11-30
+//   * forward-only half-table kernel  src/kernels/gamma_smc_flow.cu:1136-1256
+//     (run_fwd, src/bindings.cpp:2794-2849)
 //
 // Build: see oracle/Makefile (-O3 -mfma -ffp-contract=off -fopenmp).  The
 // builder must not contract a*b+c into FMA, because the reference's table
@@ -437,6 +439,62 @@ int oracle_fb_window(const uint64_t* packed, long long n_words,
     }
   }
   return 0;
+}
+
+// Forward-only filtered posterior (the reference's run_fwd: the half copy of
+// the hom multi-step table, src/kernels/gamma_smc_flow.cu:1136-1256).  hom_m /
+// hom_c are that table [L][2550] already rounded through float16 by the
+// caller.  exp10f / log10f / exp2f stand in for the device's __exp10f /
+// __log10f / exp2f, which differ by a few ulp.  Outputs [S][P].
+void oracle_fwd_only(const uint64_t* packed, long long n_words, const double* pos,
+                     long long S, const int* pi, const int* pj, long long P, float two_ne,
+                     const float* hom_m, const float* hom_c, int L, float* mean,
+                     float* lower, float* upper, int n_threads) {
+#ifdef _OPENMP
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+#else
+  (void)n_threads;
+#endif
+#pragma omp parallel for schedule(dynamic, 16)
+  for (long long p = 0; p < P; ++p) {
+    const uint64_t* hi = packed + (long long)pi[p] * n_words;
+    const uint64_t* hj = packed + (long long)pj[p] * n_words;
+    float m = 0.0f, c = 0.0f;
+    double prev = 0.0;
+    for (long long s = 0; s < S; ++s) {
+      const double x = pos[s];
+      const double g = x - prev + 0.5;
+      int gap = g >= 2147483647.0 ? 2147483647 : (int)g;  // truncation, as the reference
+      prev = x;
+      if (s > 0 && gap > 0) {
+        while (gap > L) {
+          layer_apply(hom_m, hom_c, L - 1, m, c);
+          gap -= L;
+        }
+        layer_apply(hom_m, hom_c, gap - 1, m, c);
+      }
+      if ((((hi[s >> 6] ^ hj[s >> 6]) >> (s & 63)) & 1u) != 0) {
+        const float alpha = exp10f(-2.0f * c) + 1.0f;
+        const float a_log = log10f(alpha);
+        const float b_log = fmaf(-2.0f, c, -m);
+        m = a_log - b_log;
+        c = -0.5f * a_log;
+      }
+      const float mg = exp2f(m * 3.321928094887362f) * two_ne;
+      const size_t o = (size_t)s * P + p;
+      mean[o] = mg;
+      if (lower && upper) {
+        const float alpha = exp10f(-2.0f * c);
+        const float inv9a = 1.0f / (9.0f * alpha);
+        const float sq = sqrtf(inv9a);
+        const float base = 1.0f - inv9a;
+        const float lo = fmaxf(fmaf(-1.96f, sq, base), 0.0f);
+        const float up = fmaf(1.96f, sq, base);
+        lower[o] = fmaxf(mg * lo * lo * lo, 0.0f);
+        upper[o] = mg * up * up * up;
+      }
+    }
+  }
 }
 
 }  // extern "C"

@@ -79,6 +79,10 @@ def lib():
             ctypes.c_longlong, _i32p, _i32p, ctypes.c_longlong, ctypes.c_float,
             _f32p, ctypes.c_int, _f32p, _f32p, _f32p, _f32p, _f32p, ctypes.c_int]
         L.oracle_fb_window.restype = ctypes.c_int
+        L.oracle_fwd_only.argtypes = [
+            _u64p, ctypes.c_longlong, _f64p, ctypes.c_longlong, _i32p, _i32p, ctypes.c_longlong,
+            ctypes.c_float, _f32p, _f32p, ctypes.c_int, _f32p, _f32p, _f32p, ctypes.c_int]
+        L.oracle_fwd_only.restype = None
         L.oracle_layer_bilinear.argtypes = [_f32p, ctypes.c_float, ctypes.c_float]
         L.oracle_layer_bilinear.restype = ctypes.c_float
         _lib = L
@@ -382,3 +386,46 @@ def infer_blockwise(G_or_ts, positions=None, mu=1.25e-8, rho=1e-8, Ne=10000, pai
     r["pairs"] = pairs
     r["positions"] = positions
     return r
+
+
+def run_fb_summary(G, positions, pairs, Ne, mu, rho, flow_field_path, core_block_sites=0,
+                   flank_sites=2048, n_threads=0):
+    """Per-site mean / min / max over pairs of the posterior mean
+    (FlowContext.run_fb_summary, src/bindings.cpp:2695-2788): the per-pair
+    means of the full-sequence (or blockwise) scan, averaged in float64."""
+    S = G.shape[1]
+    if core_block_sites and 0 < core_block_sites < S:
+        r = run_fb_blockwise(G, positions, pairs, Ne, mu, rho, flow_field_path,
+                             core_block_sites, flank_sites, True, False, n_threads)
+    else:
+        r = run_fb(G, positions, pairs, Ne, mu, rho, flow_field_path, True, False, n_threads)
+    m = r["mean"]
+    return {"site_mean": (m.astype(np.float64).sum(axis=1) / m.shape[1]).astype(np.float32),
+            "site_min": m.min(axis=1), "site_max": m.max(axis=1), "n_pairs": m.shape[1]}
+
+
+def run_fwd(G, positions, pairs, Ne, mu, rho, flow_field_path, mean_only=True, n_threads=0):
+    """FlowContext(...).run_fwd(...) on the CPU: the forward-only filtered
+    posterior of src/kernels/gamma_smc_flow.cu:1136-1256 on the hom
+    multi-step table rounded through float16 (src/bindings.cpp:2098-2107)."""
+    S = G.shape[1]
+    T = tables_for(flow_field_path, Ne, mu, rho)
+    hom_m = np.ascontiguousarray(T[2].astype(np.float16).astype(np.float32))
+    hom_c = np.ascontiguousarray(T[3].astype(np.float16).astype(np.float32))
+    packed = bitpack(G)
+    pi = np.ascontiguousarray([p[0] for p in pairs], np.int32)
+    pj = np.ascontiguousarray([p[1] for p in pairs], np.int32)
+    P = len(pi)
+    positions = np.ascontiguousarray(positions, np.float64)
+    out = {"mean": np.empty((S, P), np.float32)}
+    if not mean_only:
+        out["lower"] = np.empty((S, P), np.float32)
+        out["upper"] = np.empty((S, P), np.float32)
+    if P == 0 or S == 0:
+        return out
+    lib().oracle_fwd_only(
+        _ptr(packed, _u64p), packed.shape[1], _ptr(positions, _f64p), S, _ptr(pi, _i32p),
+        _ptr(pj, _i32p), P, float(np.float32(2.0 * np.float32(Ne))), _ptr(hom_m, _f32p),
+        _ptr(hom_c, _f32p), hom_m.shape[0], _ptr(out["mean"], _f32p),
+        _ptr(out.get("lower"), _f32p), _ptr(out.get("upper"), _f32p), int(n_threads))
+    return out

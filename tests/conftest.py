@@ -45,3 +45,18 @@ def oracle():
 def small_data():
     from gamma_smc_cu_b200 import synthetic
     return synthetic.cohort("small")
+
+
+@pytest.fixture(scope="session")
+def ref_core():
+    """The reference's own pybind11 module built from its sources for sm_100a
+    into oracle/_ref (None when absent); loaded once per process."""
+    import importlib.util
+    from oracle import oracle as O
+    path = O.ref_core_path()
+    if path is None:
+        return None
+    spec = importlib.util.spec_from_file_location("_core", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod

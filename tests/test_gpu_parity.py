@@ -208,21 +208,10 @@ def test_device_entry_point_matches_host(small, flow_field):
         assert (o[:, :pad] == -1.0).all()
 
 
-def _ref_core():
-    from oracle import oracle as O
-    path = O.ref_core_path()
-    if path is None:
-        return None
-    spec = importlib.util.spec_from_file_location("_core", path)
-    mod = importlib.util.module_from_spec(spec)
-    spec.loader.exec_module(mod)
-    return mod
-
-
-def test_oracle_and_cuda_match_reference_gpu_build(small, oracle, flow_field):
+def test_oracle_and_cuda_match_reference_gpu_build(small, oracle, flow_field, ref_core):
     """The reference's own _core (compiled from its sources for sm_100a into
     oracle/_ref) on the same inputs: pins the oracle's scan restatement."""
-    ref = _ref_core()
+    ref = ref_core
     if ref is None:
         pytest.skip("reference _core not built in oracle/_ref")
     G, pos, mu, rho = small

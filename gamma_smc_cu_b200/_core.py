@@ -65,6 +65,19 @@ def unpack(packed, n, S):
     return out
 
 
+def diploid_het_counts(G):
+    """int64 [n_haps // 2]: sites where haplotypes 2k and 2k+1 differ, counted
+    on the GPU (bit-packed XOR + popcount); the calibration sums of
+    infer.py:44-99."""
+    G = np.ascontiguousarray(G, dtype=np.uint8)
+    if G.ndim != 2:
+        raise ValueError("G must be 2D (n_haplotypes x n_sites)")
+    n, S = G.shape
+    out = np.zeros(n // 2, np.int64)
+    check(_lib.load().gsmc_diploid_het_counts(ptr(G, _lib.c_u8p), n, S, ptr(out, _lib.c_i64p)))
+    return out
+
+
 def _split_pairs(pairs):
     """List of (i, j) (or an (P, 2) array) -> two contiguous int32 arrays."""
     if isinstance(pairs, np.ndarray):

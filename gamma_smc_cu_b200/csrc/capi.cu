@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "ctx_view.h"
+#include "flowgen.h"
 #include "fwd.h"
 #include "gsmc_b200.h"
 #include "hostcopy.h"
@@ -1003,6 +1004,49 @@ int gsmc_copy_to_host(int64_t n, void* const* dst, const void* const* src, const
   return GSMC_OK;
 }
 
+int gsmc_generate_flow_field(const double* alpha, const double* beta, int mean_n, int cv_n,
+                             int n_steps, int n_epochs, const double* epoch_start,
+                             const double* epoch_rate, const double* epoch_cum,
+                             double calibration, double* u, double* v) {
+  if (mean_n <= 0 || cv_n <= 0 || !alpha || !beta || !u || !v)
+    return fail(GSMC_E_INVALID, "bad flow-field grid");
+  if (n_steps < 2 || flow_field_smem_bytes(n_steps) > 200 * 1024)
+    return fail(GSMC_E_INVALID, "n_steps must be in [2, 2559]");
+  if (n_epochs < 0 || n_epochs > kMaxEpochs)
+    return fail(GSMC_E_INVALID, "at most %d epochs are supported", kMaxEpochs);
+  if (n_epochs > 0 && (!epoch_start || !epoch_rate || !epoch_cum))
+    return fail(GSMC_E_INVALID, "null epoch arrays");
+  FlowGenEpochs ep;
+  std::memset(&ep, 0, sizeof(ep));
+  ep.n = n_epochs;
+  for (int k = 0; k < n_epochs; ++k) {
+    ep.t_bounds[k] = epoch_start[k];
+    ep.lam[k] = epoch_rate[k];
+    ep.L_bounds[k] = epoch_cum[k];
+  }
+  const size_t cells = (size_t)mean_n * cv_n;
+  double* d = nullptr;
+  CUDA_TRY(cudaMalloc(&d, 4 * cells * sizeof(double)));
+  FlowGenArgs a;
+  a.alpha = d;
+  a.beta = d + cells;
+  a.u = d + 2 * cells;
+  a.v = d + 3 * cells;
+  a.mean_n = mean_n;
+  a.cv_n = cv_n;
+  a.n_steps = n_steps;
+  a.t_max_exp = -std::log(1e-3);
+  a.calibration = calibration;
+  cudaError_t e = cudaMemcpy(d, alpha, cells * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + cells, beta, cells * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = launch_flow_field(a, ep, nullptr);
+  if (e == cudaSuccess) e = cudaMemcpy(u, a.u, cells * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(v, a.v, cells * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(GSMC_E_CUDA, "CUDA error: %s (flow field)", cudaGetErrorString(e));
+  return GSMC_OK;
+}
+
 int gsmc_bitpack(const uint8_t* G, int64_t n_haps, int64_t n_sites, uint64_t* packed) {
   if (n_haps < 0 || n_sites < 0) return fail(GSMC_E_INVALID, "negative shape");
   if (n_haps > 65535) return fail(GSMC_E_INVALID, "at most 65535 haplotypes are supported");
@@ -1018,6 +1062,35 @@ int gsmc_bitpack(const uint8_t* G, int64_t n_haps, int64_t n_sites, uint64_t* pa
   cudaFree(dG);
   cudaFree(dP);
   if (e != cudaSuccess) return fail(GSMC_E_CUDA, "CUDA error: %s (bitpack)", cudaGetErrorString(e));
+  return GSMC_OK;
+}
+
+int gsmc_diploid_het_counts(const uint8_t* G, int64_t n_haps, int64_t n_sites, int64_t* counts) {
+  if (n_haps < 0 || n_sites < 0) return fail(GSMC_E_INVALID, "negative shape");
+  if (n_haps > 65535) return fail(GSMC_E_INVALID, "at most 65535 haplotypes are supported");
+  const int64_t nd = n_haps / 2;
+  if (nd == 0) return GSMC_OK;
+  if (!counts || (n_sites > 0 && !G)) return fail(GSMC_E_INVALID, "null array");
+  if (n_sites == 0) {
+    std::fill(counts, counts + nd, (int64_t)0);
+    return GSMC_OK;
+  }
+  const int64_t groups = (n_sites + 127) / 128;
+  uint8_t* dG = nullptr;
+  ulonglong2* dP = nullptr;
+  long long* dC = nullptr;
+  CUDA_TRY(cudaMalloc(&dG, (size_t)n_haps * n_sites));
+  cudaError_t e = cudaMalloc(&dP, (size_t)groups * n_haps * sizeof(ulonglong2));
+  if (e == cudaSuccess) e = cudaMalloc(&dC, (size_t)nd * sizeof(long long));
+  if (e == cudaSuccess) e = cudaMemset(dP, 0, (size_t)groups * n_haps * sizeof(ulonglong2));
+  if (e == cudaSuccess) e = cudaMemcpy(dG, G, (size_t)n_haps * n_sites, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = launch_bitpack(dG, n_haps, n_sites, dP, true, nullptr);
+  if (e == cudaSuccess) e = launch_het_counts(dP, n_haps, groups, dC, nullptr);
+  if (e == cudaSuccess) e = cudaMemcpy(counts, dC, (size_t)nd * sizeof(long long), cudaMemcpyDeviceToHost);
+  cudaFree(dG);
+  cudaFree(dP);
+  cudaFree(dC);
+  if (e != cudaSuccess) return fail(GSMC_E_CUDA, "CUDA error: %s (het counts)", cudaGetErrorString(e));
   return GSMC_OK;
 }
 

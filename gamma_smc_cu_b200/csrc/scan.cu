@@ -123,6 +123,29 @@ __global__ void summary_finish_kernel(const double* __restrict__ acc_sum, int64_
   if (s < rows) site_mean[s] = (float)(acc_sum[s] / n_pairs);
 }
 
+// counts[k] = popcount of the XOR of haplotypes 2k and 2k+1 over all
+// 128-site groups (bits past the last site are zero in both).  One CTA per
+// diploid; int64 partial sums in a fixed order.
+__global__ void het_count_kernel(const ulonglong2* __restrict__ geno, int64_t n_haps,
+                                 int64_t n_groups, long long* __restrict__ counts) {
+  const int64_t k = blockIdx.x;
+  __shared__ long long part[32];
+  long long n = 0;
+  for (int64_t g = threadIdx.x; g < n_groups; g += blockDim.x) {
+    const ulonglong2 a = geno[g * n_haps + 2 * k], b = geno[g * n_haps + 2 * k + 1];
+    n += __popcll(a.x ^ b.x) + __popcll(a.y ^ b.y);
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) n += __shfl_xor_sync(0xffffffffu, n, d);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = n;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += part[w];
+    counts[k] = t;
+  }
+}
+
 // Pack genotypes: thread (h, word) builds 64 sites of haplotype h.
 template <bool SCAN_LAYOUT>
 __global__ void bitpack_kernel(const uint8_t* __restrict__ G, int64_t n, int64_t S,
@@ -231,6 +254,13 @@ cudaError_t launch_summary_finish(const double* acc_sum, int64_t rows, double n_
   if (rows <= 0) return cudaSuccess;
   summary_finish_kernel<<<(unsigned)((rows + 255) / 256), 256, 0, stream>>>(acc_sum, rows, n_pairs,
                                                                            site_mean);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_het_counts(const ulonglong2* geno, int64_t n_haps, int64_t n_groups,
+                              long long* counts, cudaStream_t stream) {
+  if (n_haps < 2 || n_groups <= 0) return cudaSuccess;
+  het_count_kernel<<<(unsigned)(n_haps / 2), 256, 0, stream>>>(geno, n_haps, n_groups, counts);
   return cudaGetLastError();
 }
 

@@ -103,6 +103,10 @@ cudaError_t launch_summary_fold(const float* p_sum, const float* p_min, const fl
 cudaError_t launch_summary_finish(const double* acc_sum, int64_t rows, double n_pairs,
                                   float* site_mean, cudaStream_t stream);
 
+// counts[k] = sites where haplotypes 2k and 2k+1 differ (scan layout input).
+cudaError_t launch_het_counts(const ulonglong2* geno, int64_t n_haps, int64_t n_groups,
+                              long long* counts, cudaStream_t stream);
+
 // Pack [n_haps x n_sites] uint8 genotypes.  scan_layout: word-major 128-site
 // groups for the scan; otherwise the reference's row-major uint64 words.
 cudaError_t launch_bitpack(const uint8_t* G, int64_t n_haps, int64_t n_sites, void* out,

@@ -41,29 +41,38 @@ def _coerce_inputs(G_or_ts, positions):
     return G, pos
 
 
-def _estimate_scaled_params(G, positions, mu, rho, Ne):
-    """Data-driven (effective_mu, effective_rho) as gamma_smc's auto mode sets
-    them (infer.py:44-99).
+def _scaled_params_from_counts(het_per_individual, positions, mu, rho, Ne):
+    """(effective_mu, effective_rho) from per-diploid het counts (infer.py:44-99).
 
     The scaled mutation rate is the mean per-diploid heterozygosity over the
-    span [0, last position + 1): haplotypes 2k and 2k+1 form individual k.  The
-    scaled recombination rate keeps the user's rho/mu ratio.  Both are returned
-    divided by 4 Ne so that 4 Ne * rate reproduces them.  The raw (mu, rho) come
-    back unchanged for n < 2, odd n, no sites, or a non-positive estimate.
+    span [0, last position + 1); the scaled recombination rate keeps the
+    user's rho/mu ratio; both are returned divided by 4 Ne so that 4 Ne * rate
+    reproduces them.  The raw (mu, rho) come back for a non-positive span or
+    estimate.
     """
-    n, S = G.shape
-    if n < 2 or S == 0 or n % 2:
-        return float(mu), float(rho)
     span = float(positions[-1] + 1.0)
     if span <= 0:
         return float(mu), float(rho)
-    het_per_individual = np.count_nonzero(G[0::2] != G[1::2], axis=1).astype(np.int64)
-    pi_hat = float(het_per_individual.mean()) / span
+    pi_hat = float(np.asarray(het_per_individual, np.int64).mean()) / span
     if not (pi_hat > 0 and math.isfinite(pi_hat)):
         return float(mu), float(rho)
     four_ne = 4.0 * float(Ne)
     ratio = float(rho) / max(float(mu), 1e-30)
     return float(pi_hat / four_ne), float(pi_hat * ratio / four_ne)
+
+
+def _estimate_scaled_params(G, positions, mu, rho, Ne):
+    """Data-driven (effective_mu, effective_rho) as gamma_smc's auto mode sets
+    them (infer.py:44-99), counting on the host: haplotypes 2k and 2k+1 form
+    individual k.  The raw (mu, rho) come back unchanged for n < 2, odd n, no
+    sites, or a non-positive estimate.  ``infer`` makes the same counts on the
+    GPU (``_core.diploid_het_counts``); both give identical int64 counts.
+    """
+    n, S = G.shape
+    if n < 2 or S == 0 or n % 2:
+        return float(mu), float(rho)
+    het_per_individual = np.count_nonzero(G[0::2] != G[1::2], axis=1).astype(np.int64)
+    return _scaled_params_from_counts(het_per_individual, positions, mu, rho, Ne)
 
 
 def _filter_segregating(G, positions):
@@ -134,9 +143,16 @@ def _recommend_core_block_size(n_sites, n_pairs, mean_only, flank_sites, free_by
 
 
 def _scaled_rates(G, positions, mu, rho, Ne, auto_estimate_theta):
-    if auto_estimate_theta:
-        return _estimate_scaled_params(G, positions, mu, rho, Ne)
-    return float(mu), float(rho)
+    """Rates for the context: the chromosome-wide calibration counts are made
+    on the GPU from bit-packed genotypes (``_core.diploid_het_counts``,
+    looked up at call time), the rest as in _estimate_scaled_params."""
+    from gamma_smc_cu_b200 import _core
+    if not auto_estimate_theta:
+        return float(mu), float(rho)
+    n, S = G.shape
+    if n < 2 or S == 0 or n % 2:
+        return float(mu), float(rho)
+    return _scaled_params_from_counts(_core.diploid_het_counts(G), positions, mu, rho, Ne)
 
 
 def infer(G_or_ts, positions=None, mu=1.25e-8, rho=1e-8, Ne=10000, pairs=None,

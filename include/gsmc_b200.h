@@ -281,6 +281,32 @@ int gsmc_ctx_timing_read(gsmc_ctx* ctx, double* kernel_ms, int64_t* launches,
                          double* pair_sites);
 
 /*
+ * Per-diploid heterozygous site counts on the device: counts[k] = number of
+ * sites where haplotypes 2k and 2k+1 differ, k < n_haps / 2 (int64, exact),
+ * from bit-packed genotypes (XOR + popcount).  The chromosome-wide sums of
+ * the theta/rho auto-calibration, _estimate_scaled_params
+ * (python/gamma_smc_cu/infer.py:44-99), which counts with numpy.
+ */
+int gsmc_diploid_het_counts(const uint8_t* G, int64_t n_haps, int64_t n_sites, int64_t* counts);
+
+/*
+ * Flow field on the GPU in float64: for every cell of a mean_n x cv_n grid
+ * with Gamma(alpha[c], beta[c]), the least-squares drift (u[c], v[c]) of
+ * (log10 mean, log10 CV) per unit of scaled time, divided by `calibration`
+ * (the reference uses 5.302).  n_epochs = 0 is constant Ne; otherwise epoch
+ * k of a piecewise-constant N(t) starts at scaled time epoch_start[k] with
+ * coalescence rate epoch_rate[k] (Ne_ref / N_k) and cumulative rate
+ * epoch_cum[k].  Time grid of 2 n_steps + 1 points.  Cells the reference
+ * skips or cannot fit are 0.
+ * Replaces generate_flow_field (python/gamma_smc_cu/demographic.py:146-208)
+ * and its distribution-difference helpers (:17-143), which run on the CPU.
+ */
+int gsmc_generate_flow_field(const double* alpha, const double* beta, int mean_n, int cv_n,
+                             int n_steps, int n_epochs, const double* epoch_start,
+                             const double* epoch_rate, const double* epoch_cum,
+                             double calibration, double* u, double* v);
+
+/*
  * Bit-pack genotypes on the device: packed[h * n_words + w] bit b =
  * G[h][64w + b] & 1, n_words = ceil(n_sites / 64); host in, host out.
  * Replaces _core.bitpack / bitpack_kernel (src/kernels/bitpack.cu:11-38).

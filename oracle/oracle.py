@@ -218,6 +218,13 @@ def coerce_inputs(G_or_ts, positions):
     return G, pos
 
 
+def diploid_het_counts(G):
+    """int64 [n // 2]: sites where haplotypes 2k and 2k+1 differ (infer.py:77)."""
+    G = np.asarray(G)
+    n = G.shape[0] // 2 * 2
+    return np.count_nonzero(G[0:n:2] != G[1:n:2], axis=1).astype(np.int64)
+
+
 def estimate_scaled_params(G, positions, mu, rho, Ne):
     n, S = G.shape
     if n < 2 or S == 0 or n % 2 != 0:

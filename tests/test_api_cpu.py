@@ -13,6 +13,15 @@ import gamma_smc_cu_b200
 from gamma_smc_cu_b200 import synthetic
 
 
+@pytest.fixture(autouse=True)
+def host_het_counts(monkeypatch):
+    """infer() makes its calibration counts on the GPU; without one, the
+    oracle's host counts stand in (the GPU tests check they are identical)."""
+    from oracle import oracle as O
+    monkeypatch.setattr(gamma_smc_cu_b200._core, "diploid_het_counts",
+                        lambda G: O.diploid_het_counts(G))
+
+
 @pytest.fixture(scope="module")
 def genotype_data():
     pos = synthetic.positions_for(177, 1.0e5, 42)

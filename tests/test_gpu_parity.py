@@ -250,3 +250,18 @@ def test_chromosome_shape_sampled_pairs(oracle, flow_field):
                                   return_posterior=True)
     for k in KEYS:
         assert np.array_equal(got[k][:, sel], want[k]), k
+
+
+def test_gpu_calibration_counts_match_host(oracle):
+    """The per-diploid het counts infer() makes on the GPU equal the host
+    counts exactly, so the calibrated rates are identical."""
+    from gamma_smc_cu_b200.infer import _estimate_scaled_params, _scaled_rates
+    for name, S in (("small", None), ("chrom", 30000)):
+        G, pos = synthetic.cohort(name, n_sites=S)
+        got = _core.diploid_het_counts(G)
+        assert got.dtype == np.int64 and np.array_equal(got, oracle.diploid_het_counts(G))
+        assert _scaled_rates(G, pos, 1.25e-8, 1e-8, NE, True) == \
+            _estimate_scaled_params(G, pos, 1.25e-8, 1e-8, NE)
+    G = (np.random.default_rng(3).random((7, 333)) < 0.5).astype(np.uint8)  # odd n, ragged S
+    assert np.array_equal(_core.diploid_het_counts(G), oracle.diploid_het_counts(G))
+    assert _core.diploid_het_counts(np.zeros((6, 0), np.uint8)).tolist() == [0, 0, 0]

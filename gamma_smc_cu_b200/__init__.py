@@ -5,7 +5,8 @@ Drop-in for ``gamma_smc_cu.infer`` / ``infer_blockwise`` and the
 kernels in ``lib/libgsmc_b200.so`` (C ABI in ``include/gsmc_b200.h``).
 """
 from . import _core
-from ._core import FlowContext, bitpack, cuda_mem_info, get_device, get_device_count, set_device, unpack
+from ._core import (FlowContext, bitpack, cuda_mem_info, gamma_smc_flow_fb, get_device,
+                    get_device_count, set_device, unpack)
 from .infer import infer, infer_blockwise
 
 __all__ = [
@@ -13,6 +14,7 @@ __all__ = [
     "bitpack",
     "unpack",
     "cuda_mem_info",
+    "gamma_smc_flow_fb",
     "get_device",
     "get_device_count",
     "set_device",

@@ -78,6 +78,32 @@ def diploid_het_counts(G):
     return out
 
 
+def gamma_smc_flow_fb(G, positions, pairs, Ne=10000.0, mu=1.25e-8, rho=1e-8,
+                      flow_field_path=DEFAULT_FLOW_FIELD, mean_only=False):
+    """Uncached flow-field forward-backward (the reference's module-level
+    ``gamma_smc_flow_fb``, src/bindings.cpp:2159-2300): every gap integrated on
+    the flow field staged in shared memory, raw (mu, rho).  Dict with ``mean``
+    (and ``lower``/``upper`` unless mean_only), [n_sites, n_pairs] float32."""
+    G = np.ascontiguousarray(G, dtype=np.uint8)
+    positions = np.ascontiguousarray(positions, dtype=np.float64)
+    if G.ndim != 2 or positions.ndim != 1 or positions.shape[0] != G.shape[1]:
+        raise ValueError("G must be [n_haplotypes, n_sites] and positions [n_sites]")
+    n, S = G.shape
+    pi, pj = _split_pairs(pairs)
+    P = len(pi)
+    out = {"mean": np.empty((S, P), np.float32)}
+    if not mean_only:
+        out["lower"] = np.empty((S, P), np.float32)
+        out["upper"] = np.empty((S, P), np.float32)
+    check(_lib.load().gsmc_flow_fb(
+        ptr(G, _lib.c_u8p), n, S, ptr(positions, _lib.c_f64p), ptr(pi, _lib.c_i32p),
+        ptr(pj, _lib.c_i32p), P, float(Ne), float(mu), float(rho),
+        os.fsencode(str(flow_field_path)), 0 if mean_only else GSMC_CI,
+        ptr(out["mean"], _lib.c_f32p), ptr(out.get("lower"), _lib.c_f32p),
+        ptr(out.get("upper"), _lib.c_f32p)))
+    return out
+
+
 def _split_pairs(pairs):
     """List of (i, j) (or an (P, 2) array) -> two contiguous int32 arrays."""
     if isinstance(pairs, np.ndarray):

@@ -106,6 +106,9 @@ SIGNATURES = {
     "gsmc_diploid_het_counts": (c_int, [c_u8p, c_i64, c_i64, c_i64p]),
     "gsmc_generate_flow_field": (c_int, [c_f64p, c_f64p, c_int, c_int, c_int, c_int, c_f64p,
                                          c_f64p, c_f64p, ctypes.c_double, c_f64p, c_f64p]),
+    "gsmc_flow_fb": (c_int, [c_u8p, c_i64, c_i64, c_f64p, c_i32p, c_i32p, c_i64, ctypes.c_double,
+                             ctypes.c_double, ctypes.c_double, ctypes.c_char_p, c_int, c_f32p,
+                             c_f32p, c_f32p]),
     "gsmc_ctx_scratch_bytes": (c_int, [c_vp, c_u64p]),
     "gsmc_ctx_timing": (c_int, [c_vp, c_int]),
     "gsmc_ctx_timing_read": (c_int, [c_vp, ctypes.POINTER(ctypes.c_double), c_i64p,

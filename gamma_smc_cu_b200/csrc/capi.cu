@@ -22,6 +22,7 @@
 #include "hostcopy.h"
 #include "scan.h"
 #include "tables.h"
+#include "uncached.h"
 
 using namespace gsmc;
 
@@ -1044,6 +1045,139 @@ int gsmc_generate_flow_field(const double* alpha, const double* beta, int mean_n
   if (e == cudaSuccess) e = cudaMemcpy(v, a.v, cells * sizeof(double), cudaMemcpyDeviceToHost);
   cudaFree(d);
   if (e != cudaSuccess) return fail(GSMC_E_CUDA, "CUDA error: %s (flow field)", cudaGetErrorString(e));
+  return GSMC_OK;
+}
+
+int gsmc_flow_fb(const uint8_t* G, int64_t n_haps, int64_t n_sites, const double* positions,
+                 const int32_t* pair_i, const int32_t* pair_j, int64_t n_pairs, double Ne,
+                 double mu, double rho, const char* flow_field_path, int flags, float* mean,
+                 float* lower, float* upper) {
+  if (n_haps < 0 || n_sites < 0 || n_pairs < 0) return fail(GSMC_E_INVALID, "negative shape");
+  if (n_haps > 65535) return fail(GSMC_E_INVALID, "at most 65535 haplotypes are supported");
+  if (n_sites > 0x7fffffff) return fail(GSMC_E_INVALID, "too many sites");
+  const bool ci = (flags & GSMC_CI) != 0;
+  if (!flow_field_path) return fail(GSMC_E_INVALID, "null flow field path");
+  if (n_pairs == 0 || n_sites == 0) return GSMC_OK;
+  if (!G || !positions || !pair_i || !pair_j || !mean || (ci && (!lower || !upper)))
+    return fail(GSMC_E_INVALID, "null input or output array");
+  for (int64_t p = 0; p < n_pairs; ++p)
+    if (pair_i[p] < 0 || pair_i[p] >= n_haps || pair_j[p] < 0 || pair_j[p] >= n_haps)
+      return fail(GSMC_E_INVALID, "pair %lld = (%d, %d) is out of range for %lld haplotypes",
+                  (long long)p, pair_i[p], pair_j[p], (long long)n_haps);
+  FlowField ff;
+  char err[512];
+  if (load_flow_field(flow_field_path, &ff, err, sizeof(err)) != 0)
+    return fail(GSMC_E_IO, "%s", err);
+  // rates as the reference's launcher forms them in float
+  // (src/kernels/gamma_smc_flow.cu:342-344)
+  const float ne = (float)Ne, fmu = (float)mu, frho = (float)rho;
+  const float lambda = 1.0f / (2.0f * ne);
+  const float srho = 4.0f * ne * frho;
+  const float smu = 2.0f * fmu / lambda;
+  std::vector<float2> flow(kCells);
+  for (int i = 0; i < kCells; ++i) flow[i] = make_float2(ff.u[i], ff.v[i]);
+  std::vector<int> seg((size_t)n_sites);
+  for (int64_t s2 = 0; s2 < n_sites; ++s2)
+    seg[s2] = seg_steps(s2 == 0 ? positions[0] + 1.0 : positions[s2] - positions[s2 - 1]);
+  const int64_t groups = (n_sites + 127) / 128;
+  // pair chunk: forward states (8 B) + outputs per pair-site within the budget
+  const int nout = ci ? 3 : 1;
+  const size_t per_pair = (size_t)n_sites * (8 + 4 * nout);
+  const size_t budget = (size_t)(0.6 * (double)free_device_bytes());
+  int64_t chunk = std::min<int64_t>(n_pairs, std::max<int64_t>(1, (int64_t)(budget / per_pair)));
+  if (chunk < n_pairs) chunk = std::max<int64_t>(256, chunk / 256 * 256);
+  struct Bufs {
+    uint8_t* G = nullptr;
+    ulonglong2* geno = nullptr;
+    int* seg = nullptr;
+    float2* flow = nullptr;
+    int32_t* pairs = nullptr;
+    float2* fwd = nullptr;
+    float* out = nullptr;
+    int* error = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    ~Bufs() {
+      if (st) cudaStreamSynchronize(st);
+      cudaFree(G);
+      cudaFree(geno);
+      cudaFree(seg);
+      cudaFree(flow);
+      cudaFree(pairs);
+      cudaFree(fwd);
+      cudaFree(out);
+      cudaFree(error);
+      if (done) cudaEventDestroy(done);
+      if (st) cudaStreamDestroy(st);
+    }
+  } b;
+  CUDA_TRY(cudaStreamCreateWithFlags(&b.st, cudaStreamNonBlocking));
+  CUDA_TRY(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming));
+  CUDA_TRY(cudaMalloc(&b.G, (size_t)n_haps * n_sites));
+  CUDA_TRY(cudaMalloc(&b.geno, (size_t)groups * n_haps * sizeof(ulonglong2)));
+  CUDA_TRY(cudaMalloc(&b.seg, seg.size() * sizeof(int)));
+  CUDA_TRY(cudaMalloc(&b.flow, flow.size() * sizeof(float2)));
+  CUDA_TRY(cudaMalloc(&b.pairs, 2 * (size_t)n_pairs * sizeof(int32_t)));
+  CUDA_TRY(cudaMalloc(&b.error, sizeof(int)));
+  if (cudaMalloc(&b.fwd, (size_t)n_sites * chunk * sizeof(float2)) != cudaSuccess ||
+      cudaMalloc(&b.out, (size_t)n_sites * chunk * nout * sizeof(float)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(GSMC_E_NOMEM, "CUDA error: out of memory for %lld pairs x %lld sites",
+                (long long)chunk, (long long)n_sites);
+  }
+  CUDA_TRY(cudaMemsetAsync(b.geno, 0, (size_t)groups * n_haps * sizeof(ulonglong2), b.st));
+  CUDA_TRY(cudaMemsetAsync(b.error, 0, sizeof(int), b.st));
+  CUDA_TRY(cudaMemcpyAsync(b.G, G, (size_t)n_haps * n_sites, cudaMemcpyHostToDevice, b.st));
+  CUDA_TRY(launch_bitpack(b.G, n_haps, n_sites, b.geno, true, b.st));
+  CUDA_TRY(cudaMemcpyAsync(b.seg, seg.data(), seg.size() * sizeof(int), cudaMemcpyHostToDevice, b.st));
+  CUDA_TRY(cudaMemcpyAsync(b.flow, flow.data(), flow.size() * sizeof(float2), cudaMemcpyHostToDevice,
+                           b.st));
+  CUDA_TRY(cudaMemcpyAsync(b.pairs, pair_i, n_pairs * sizeof(int32_t), cudaMemcpyHostToDevice, b.st));
+  CUDA_TRY(cudaMemcpyAsync(b.pairs + n_pairs, pair_j, n_pairs * sizeof(int32_t),
+                           cudaMemcpyHostToDevice, b.st));
+  CUDA_TRY(cudaStreamSynchronize(b.st));  // host sources may go away after this call
+  HostCopier* copier = HostCopier::for_current_device();
+  if (!copier) return fail(GSMC_E_CUDA, "CUDA error: no device for the host copier");
+  float* host[3] = {mean, lower, upper};
+  int first = GSMC_OK;
+  for (int64_t off = 0; off < n_pairs && first == GSMC_OK; off += chunk) {
+    const int64_t n = std::min(chunk, n_pairs - off);
+    int e = copier->drain();  // the previous chunk's copies have read the outputs
+    UncachedArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.geno = b.geno;
+    a.n_haps = n_haps;
+    a.seg = b.seg;
+    a.flow = b.flow;
+    a.n_sites = (int)n_sites;
+    a.pi = b.pairs + off;
+    a.pj = b.pairs + n_pairs + off;
+    a.n_pairs = (int)n;
+    a.rho = srho;
+    a.mu = smu;
+    a.unscale = 2.0f * ne;
+    a.fwd = b.fwd;
+    a.mean = b.out;
+    a.lower = ci ? b.out + (size_t)n_sites * n : nullptr;
+    a.upper = ci ? b.out + (size_t)2 * n_sites * n : nullptr;
+    a.ldo = n;
+    a.error = b.error;
+    if (e == cudaSuccess) e = launch_uncached_fb(a, b.st);
+    if (e == cudaSuccess) e = cudaEventRecord(b.done, b.st);
+    for (int k = 0; k < nout && e == cudaSuccess; ++k)
+      e = copier->enqueue(host[k] + off, (size_t)n_pairs * sizeof(float),
+                          b.out + (size_t)k * n_sites * n, (size_t)n * sizeof(float),
+                          (size_t)n * sizeof(float), (size_t)n_sites, b.done);
+    if (e != cudaSuccess)
+      first = fail(GSMC_E_CUDA, "CUDA error: %s (flow FB)", cudaGetErrorString((cudaError_t)e));
+  }
+  const int e = copier->drain();
+  if (first) return first;
+  if (e != cudaSuccess)
+    return fail(GSMC_E_CUDA, "CUDA error: %s (device to host copy)", cudaGetErrorString((cudaError_t)e));
+  int flag = 0;
+  CUDA_TRY(cudaMemcpy(&flag, b.error, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag) return fail(GSMC_E_TIMEOUT, "the flow field copy into shared memory did not complete");
   return GSMC_OK;
 }
 

@@ -1,0 +1,191 @@
+// Uncached flow-field forward/backward: gamma_smc_cu.gamma_smc_flow_fb.
+//
+// Instead of the precomputed multi-step tables, every gap is integrated on
+// the flow field itself (src/kernels/gamma_smc_flow.cu:29-163, 168-398): one
+// recombination step of the per-bp rate, then ceil(10 x scaled rho of the
+// rest of the gap) sub-steps that each apply the hom emission (beta += mu)
+// and a recombination step, then the site's emission.  The backward pass
+// applies the same segment in the opposite order and combines with the
+// stored forward states like the cached scan.
+//
+// The 51 x 50 (u, v) grid -- 20,400 bytes, interleaved as float2 so a corner
+// is one 8-byte shared-memory read -- is staged once per CTA by a TMA bulk
+// copy (cp.async.bulk into shared memory, completion on an mbarrier).  The
+// wait for it is bounded: if the copy has not landed after a fixed number of
+// polls the CTA records an error and skips its pairs.  One thread per pair
+// walks all sites forward (states to a [S][P] float2 buffer) and back.
+//
+// The float arithmetic follows the reference expression by expression --
+// including the default contraction of the lines around __exp10f/__log10f --
+// so the outputs match its kernel bit for bit.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "scan_device.cuh"
+#include "uncached.h"
+
+namespace gsmc {
+namespace {
+
+constexpr int kGridCells = kRows * kCols;            // 2550
+constexpr unsigned kFlowBytes = kGridCells * sizeof(float2);  // 20400, a multiple of 16
+constexpr long long kCopyPolls = 1ll << 24;            // bounded wait for the bulk copy
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+// Stage the flow field into shared memory with one bulk copy; false if it did
+// not complete within the poll budget.
+__device__ bool stage_flow(float2* s_flow, uint64_t* bar, const float2* g_flow) {
+  const unsigned b = smem_addr(bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile(
+        "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(kFlowBytes)
+        : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_addr(s_flow)), "l"(g_flow), "r"(kFlowBytes), "r"(b)
+        : "memory");
+  }
+  uint32_t done = 0;
+  for (long long i = 0; i < kCopyPolls && !done; ++i) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(b)
+        : "memory");
+  }
+  return done != 0;
+}
+
+// Bilinear (u, v) at (m, c) from the staged grid, the scan's interpolation.
+__device__ __forceinline__ float2 flow_at(const float2* s_flow, float m, float c) {
+  float fm = __fmul_rn(__fsub_rn(m, kMLo), kMInv);
+  float fc = __fmul_rn(__fsub_rn(c, kCLo), kCInv);
+  fm = fmaxf(0.0f, fminf(fm, (float)(kRows - 1)));
+  fc = fmaxf(0.0f, fminf(fc, (float)(kCols - 1)));
+  const float rf = floorf(fminf(fm, (float)kPatchRows - 0.5f));
+  const float qf = floorf(fminf(fc, (float)kPatchCols - 0.5f));
+  const float wm = __fsub_rn(fm, rf), wc = __fsub_rn(fc, qf);
+  const int base = (int)rf * kCols + (int)qf;
+  const float2 v00 = s_flow[base], v01 = s_flow[base + 1];
+  const float2 v10 = s_flow[base + kCols], v11 = s_flow[base + kCols + 1];
+  const float vc = __fsub_rn(1.0f, wc), vm = __fsub_rn(1.0f, wm);
+  float2 r;
+  r.x = __fmaf_rn(wm, __fmaf_rn(wc, v11.x, __fmul_rn(vc, v10.x)),
+                  __fmul_rn(vm, __fmaf_rn(wc, v01.x, __fmul_rn(vc, v00.x))));
+  r.y = __fmaf_rn(wm, __fmaf_rn(wc, v11.y, __fmul_rn(vc, v10.y)),
+                  __fmul_rn(vm, __fmaf_rn(wc, v01.y, __fmul_rn(vc, v00.y))));
+  return r;
+}
+
+__device__ __forceinline__ void recomb_step(const float2* s_flow, float rho, float& m, float& c) {
+  const float2 d = flow_at(s_flow, m, c);
+  m = __fmaf_rn(d.x, rho, m);
+  c = __fmaf_rn(d.y, rho, c);
+  m = fmaxf(kMLo, fminf(m, kMHi));
+  c = fmaxf(kCLo, fminf(c, kCHi));
+}
+
+// Rest of a gap: sub-steps of at most 0.1 scaled recombination, each a hom
+// emission then a recombination step (src/kernels/gamma_smc_flow.cu:63-95).
+__device__ __forceinline__ void advance(const float2* s_flow, float rho_total, float mu_total,
+                                        float& m, float& c) {
+  if (rho_total < 1e-12f) return;
+  const int n_iter = max(1, (int)ceilf(rho_total * (1.0f / 0.1f)));
+  const float inv_n = __frcp_rn((float)n_iter);
+  const float rho_per = rho_total * inv_n;
+  const float mu_per = mu_total * inv_n;
+  for (int i = 0; i < n_iter; ++i) {
+    // as the reference writes it (default contraction around the intrinsics)
+    const float a_log = -2.0f * c;
+    float b_log = a_log - m;
+    const float b_lin = __exp10f(b_log) + mu_per;
+    b_log = __log10f(b_lin);
+    m = a_log - b_log;
+    recomb_step(s_flow, rho_per, m, c);
+  }
+}
+
+// Observed site: hom emission always, het adds alpha + 1 (:141-158).
+__device__ __forceinline__ void emit(bool het, float mu, float& m, float& c) {
+  float a_log = -2.0f * c;
+  float b_log = a_log - m;
+  b_log = __log10f(__exp10f(b_log) + mu);
+  if (het) a_log = __log10f(__exp10f(a_log) + 1.0f);
+  m = a_log - b_log;
+  c = -0.5f * a_log;
+}
+
+// The segment of `seg` base pairs entering a site: one per-bp recombination
+// step, then the rest of the gap.
+__device__ __forceinline__ void segment(const float2* s_flow, int seg, float rho, float mu,
+                                       float& m, float& c) {
+  if (rho >= 1e-12f) recomb_step(s_flow, rho, m, c);
+  if (seg > 1) advance(s_flow, rho * (float)(seg - 1), mu * (float)(seg - 1), m, c);
+}
+
+template <bool CI>
+__global__ void __launch_bounds__(256) uncached_fb_kernel(const UncachedArgs a) {
+  __shared__ __align__(16) float2 s_flow[kGridCells];
+  __shared__ __align__(8) uint64_t bar;
+  if (!stage_flow(s_flow, &bar, a.flow)) {
+    if (threadIdx.x == 0) atomicExch(a.error, 1);
+    return;
+  }
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.n_pairs) return;
+  const int hi = a.pi[p], hj = a.pj[p];
+  if (hi < 0 || hi >= a.n_haps || hj < 0 || hj >= a.n_haps) return;
+  const ulonglong2* gi = a.geno + hi;
+  const ulonglong2* gj = a.geno + hj;
+  const int S = a.n_sites;
+  const int64_t P = a.n_pairs;
+  float m = 0.0f, c = 0.0f;
+  uint64_t x = 0;
+  for (int s = 0; s < S; ++s) {
+    if ((s & 63) == 0) x = word_at(gi, a.n_haps, s) ^ word_at(gj, a.n_haps, s);
+    const bool het = (x >> (s & 63)) & 1ull;
+    segment(s_flow, a.seg[s], a.rho, a.mu, m, c);
+    emit(het, a.mu, m, c);
+    __stcs(a.fwd + (int64_t)s * P + p, make_float2(m, c));
+  }
+  m = 0.0f;
+  c = 0.0f;
+  Task t;  // output addressing for the shared combine
+  t.unscale = a.unscale;
+  t.out[0] = a.mean;
+  t.out[1] = a.lower;
+  t.out[2] = a.upper;
+  t.out[3] = t.out[4] = nullptr;
+  for (int s = S - 1; s >= 0; --s) {
+    const float2 f = __ldlu(a.fwd + (int64_t)s * P + p);
+    combine_store(t, (int64_t)s * a.ldo + p, f, m, c, CI, false);
+    if ((s & 63) == 63 || s == S - 1) x = word_at(gi, a.n_haps, s) ^ word_at(gj, a.n_haps, s);
+    const bool het = (x >> (s & 63)) & 1ull;
+    emit(het, a.mu, m, c);
+    segment(s_flow, a.seg[s], a.rho, a.mu, m, c);
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_uncached_fb(const UncachedArgs& a, cudaStream_t stream) {
+  if (a.n_pairs <= 0 || a.n_sites <= 0) return cudaSuccess;
+  const unsigned grid = (unsigned)((a.n_pairs + 255) / 256);
+  if (a.lower && a.upper)
+    uncached_fb_kernel<true><<<grid, 256, 0, stream>>>(a);
+  else
+    uncached_fb_kernel<false><<<grid, 256, 0, stream>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace gsmc

@@ -307,6 +307,22 @@ int gsmc_generate_flow_field(const double* alpha, const double* beta, int mean_n
                              double calibration, double* u, double* v);
 
 /*
+ * Uncached flow-field forward/backward for n_pairs pairs of G into HOST arrays
+ * of [n_sites x n_pairs] float32 (mean; lower/upper with GSMC_CI): every gap
+ * is integrated on the 51 x 50 flow field staged in shared memory (one
+ * per-bp recombination step, then sub-steps of at most 0.1 scaled
+ * recombination with hom emissions), no multi-step tables; rates are the raw
+ * (mu, rho) scaled by 4 Ne.  No context: G and positions are uploaded per
+ * call.  GSMC_E_TIMEOUT if the shared-memory staging did not complete.
+ * Replaces gamma_smc_flow_fb (src/bindings.cpp:2159-2300) and
+ * gamma_smc_flow_fb_gpu (src/kernels/gamma_smc_flow.cu:168-398).
+ */
+int gsmc_flow_fb(const uint8_t* G, int64_t n_haps, int64_t n_sites, const double* positions,
+                 const int32_t* pair_i, const int32_t* pair_j, int64_t n_pairs, double Ne,
+                 double mu, double rho, const char* flow_field_path, int flags, float* mean,
+                 float* lower, float* upper);
+
+/*
  * Bit-pack genotypes on the device: packed[h * n_words + w] bit b =
  * G[h][64w + b] & 1, n_words = ceil(n_sites / 64); host in, host out.
  * Replaces _core.bitpack / bitpack_kernel (src/kernels/bitpack.cu:11-38).

@@ -14,6 +14,8 @@
 //   * bitpack                         src/kernels/bitpack.cu:11-30
 //   * forward-only half-table kernel  src/kernels/gamma_smc_flow.cu:1136-1256
 //     (run_fwd, src/bindings.cpp:2794-2849)
+//   * uncached flow-field FB          src/kernels/gamma_smc_flow.cu:29-163,
+//     168-398 (gamma_smc_flow_fb, src/bindings.cpp:2159-2300)
 //
 // Build: see oracle/Makefile (-O3 -mfma -ffp-contract=off -fopenmp).  The
 // builder must not contract a*b+c into FMA, because the reference's table
@@ -492,6 +494,100 @@ void oracle_fwd_only(const uint64_t* packed, long long n_words, const double* po
         const float up = fmaf(1.96f, sq, base);
         lower[o] = fmaxf(mg * lo * lo * lo, 0.0f);
         upper[o] = mg * up * up * up;
+      }
+    }
+  }
+}
+
+// Uncached flow-field FB (gamma_smc_flow_fb): each gap integrated on the
+// 51 x 50 (u, v) grid.  u / v are the flow field [2550]; rho / mu the scaled
+// per-bp rates.  libm exp10f / log10f stand in for __exp10f / __log10f.
+namespace {
+inline float flow_bilinear(const float* t, float m, float c) { return layer_bilinear(t, m, c); }
+
+inline void o_recomb(const float* u, const float* v, float rho, float& m, float& c) {
+  const float du = flow_bilinear(u, m, c), dv = flow_bilinear(v, m, c);
+  m = fmaf(du, rho, m);
+  c = fmaf(dv, rho, c);
+  m = std::max(-5.0f, std::min(m, 2.0f));
+  c = std::max(-2.0f, std::min(c, 0.0f));
+}
+
+inline void o_segment(const float* u, const float* v, int seg, float rho, float mu, float& m,
+                      float& c) {
+  if (rho >= 1e-12f) o_recomb(u, v, rho, m, c);
+  if (seg <= 1) return;
+  const float rt = rho * (float)(seg - 1), mt = mu * (float)(seg - 1);
+  if (rt < 1e-12f) return;
+  const int n_iter = std::max(1, (int)std::ceil(rt * (1.0f / 0.1f)));
+  const float inv_n = 1.0f / (float)n_iter;
+  const float rp = rt * inv_n, mp = mt * inv_n;
+  for (int i = 0; i < n_iter; ++i) {
+    const float a_log = -2.0f * c;
+    const float b_log = log10f(exp10f(a_log - m) + mp);
+    m = a_log - b_log;
+    o_recomb(u, v, rp, m, c);
+  }
+}
+
+inline void o_emit(bool het, float mu, float& m, float& c) {
+  float a_log = -2.0f * c;
+  const float b_log = log10f(exp10f(a_log - m) + mu);
+  if (het) a_log = log10f(exp10f(a_log) + 1.0f);
+  m = a_log - b_log;
+  c = -0.5f * a_log;
+}
+}  // namespace
+
+void oracle_flow_fb(const uint64_t* packed, long long n_words, const double* pos, long long S,
+                    const int* pi, const int* pj, long long P, const float* u, const float* v,
+                    float rho, float mu, float Ne, float* mean, float* lower, float* upper,
+                    int n_threads) {
+#ifdef _OPENMP
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+#else
+  (void)n_threads;
+#endif
+  const float unscale = 2.0f * Ne;
+  std::vector<int> seg((size_t)S);
+  for (long long s = 0; s < S; ++s)
+    seg[s] = seg_steps_of(s == 0 ? pos[0] + 1.0 : pos[s] - pos[s - 1]);
+#pragma omp parallel
+  {
+    std::vector<float> fwd((size_t)S * 2);
+#pragma omp for schedule(dynamic, 16)
+    for (long long p = 0; p < P; ++p) {
+      const uint64_t* hi = packed + (long long)pi[p] * n_words;
+      const uint64_t* hj = packed + (long long)pj[p] * n_words;
+      auto het_at = [&](long long s) { return ((hi[s >> 6] ^ hj[s >> 6]) >> (s & 63)) & 1u; };
+      float m = 0.0f, c = 0.0f;
+      for (long long s = 0; s < S; ++s) {
+        o_segment(u, v, seg[s], rho, mu, m, c);
+        o_emit(het_at(s) != 0, mu, m, c);
+        fwd[2 * s] = m;
+        fwd[2 * s + 1] = c;
+      }
+      m = 0.0f;
+      c = 0.0f;
+      for (long long s = S - 1; s >= 0; --s) {
+        float ba, bb, fa, fb;
+        state_to_ab(m, c, ba, bb);
+        state_to_ab(fwd[2 * s], fwd[2 * s + 1], fa, fb);
+        const float a_s = fa + ba - 1.0f, b_s = fb + bb - 1.0f;
+        const float mg = (a_s / fmaxf(b_s, 1e-10f)) * unscale;
+        const size_t o = (size_t)s * P + p;
+        mean[o] = mg;
+        if (lower && upper) {
+          const float inv9a = 1.0f / (9.0f * fmaxf(a_s, 1.0f));
+          const float sq = sqrtf(inv9a);
+          const float base = 1.0f - inv9a;
+          const float lo = fmaxf(fmaf(-1.96f, sq, base), 0.0f);
+          lower[o] = fmaxf(mg * lo * lo * lo, 0.0f);
+          const float up = fmaf(1.96f, sq, base);
+          upper[o] = mg * up * up * up;
+        }
+        o_emit(het_at(s) != 0, mu, m, c);
+        o_segment(u, v, seg[s], rho, mu, m, c);
       }
     }
   }

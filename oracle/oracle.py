@@ -83,6 +83,11 @@ def lib():
             _u64p, ctypes.c_longlong, _f64p, ctypes.c_longlong, _i32p, _i32p, ctypes.c_longlong,
             ctypes.c_float, _f32p, _f32p, ctypes.c_int, _f32p, _f32p, _f32p, ctypes.c_int]
         L.oracle_fwd_only.restype = None
+        L.oracle_flow_fb.argtypes = [
+            _u64p, ctypes.c_longlong, _f64p, ctypes.c_longlong, _i32p, _i32p, ctypes.c_longlong,
+            _f32p, _f32p, ctypes.c_float, ctypes.c_float, ctypes.c_float, _f32p, _f32p, _f32p,
+            ctypes.c_int]
+        L.oracle_flow_fb.restype = None
         L.oracle_layer_bilinear.argtypes = [_f32p, ctypes.c_float, ctypes.c_float]
         L.oracle_layer_bilinear.restype = ctypes.c_float
         _lib = L
@@ -435,4 +440,35 @@ def run_fwd(G, positions, pairs, Ne, mu, rho, flow_field_path, mean_only=True, n
         _ptr(pj, _i32p), P, float(np.float32(2.0 * np.float32(Ne))), _ptr(hom_m, _f32p),
         _ptr(hom_c, _f32p), hom_m.shape[0], _ptr(out["mean"], _f32p),
         _ptr(out.get("lower"), _f32p), _ptr(out.get("upper"), _f32p), int(n_threads))
+    return out
+
+
+def flow_fb(G, positions, pairs, Ne, mu, rho, flow_field_path, mean_only=False, n_threads=0):
+    """gamma_smc_cu.gamma_smc_flow_fb on the CPU: the uncached flow-field FB
+    (src/kernels/gamma_smc_flow.cu:29-163, 168-398) with the launcher's float
+    rates (:342-344) and no theta calibration."""
+    S = G.shape[1]
+    u, v, _ = load_flow_field(flow_field_path)
+    u = np.ascontiguousarray(u, np.float32).ravel()
+    v = np.ascontiguousarray(v, np.float32).ravel()
+    ne, fmu, frho = np.float32(Ne), np.float32(mu), np.float32(rho)
+    lam = np.float32(1.0) / (np.float32(2.0) * ne)
+    srho = np.float32(4.0) * ne * frho
+    smu = np.float32(2.0) * fmu / lam
+    packed = bitpack(G)
+    pi = np.ascontiguousarray([p[0] for p in pairs], np.int32)
+    pj = np.ascontiguousarray([p[1] for p in pairs], np.int32)
+    P = len(pi)
+    positions = np.ascontiguousarray(positions, np.float64)
+    out = {"mean": np.empty((S, P), np.float32)}
+    if not mean_only:
+        out["lower"] = np.empty((S, P), np.float32)
+        out["upper"] = np.empty((S, P), np.float32)
+    if P == 0 or S == 0:
+        return out
+    lib().oracle_flow_fb(_ptr(packed, _u64p), packed.shape[1], _ptr(positions, _f64p), S,
+                         _ptr(pi, _i32p), _ptr(pj, _i32p), P, _ptr(u, _f32p), _ptr(v, _f32p),
+                         float(srho), float(smu), float(ne), _ptr(out["mean"], _f32p),
+                         _ptr(out.get("lower"), _f32p), _ptr(out.get("upper"), _f32p),
+                         int(n_threads))
     return out

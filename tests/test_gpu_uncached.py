@@ -1,0 +1,69 @@
+"""Uncached flow-field forward/backward (gamma_smc_flow_fb) on the GPU.
+
+Against the reference's own GPU build it must be bit-identical (same float
+arithmetic, same __exp10f/__log10f); against the CPU oracle, which uses libm
+exp10f/log10f, within the 1e-4 relative tolerance.
+"""
+import numpy as np
+import pytest
+
+import gamma_smc_cu_b200 as G200
+from gamma_smc_cu_b200 import _core, synthetic
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-4
+KEYS = ("mean", "lower", "upper")
+
+
+def _max_rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-30))) if a.size else 0.0
+
+
+def test_flow_fb_matches_oracle(small_data, oracle, flow_field):
+    G, pos = small_data
+    pairs = [(i, j) for i in range(40) for j in range(i)]
+    got = G200.gamma_smc_flow_fb(G, pos, pairs, Ne=1e4, flow_field_path=flow_field)
+    want = oracle.flow_fb(G, pos, pairs, 1e4, 1.25e-8, 1e-8, flow_field)
+    for k in KEYS:
+        assert got[k].shape == want[k].shape == (G.shape[1], len(pairs))
+        assert _max_rel(got[k], want[k]) <= RTOL, (k, _max_rel(got[k], want[k]))
+    m = G200.gamma_smc_flow_fb(G, pos, pairs[:30], Ne=1e4, flow_field_path=flow_field,
+                               mean_only=True)
+    assert set(m) == {"mean"} and np.array_equal(m["mean"], got["mean"][:, :30])
+
+
+def test_flow_fb_other_rates_and_gaps(oracle, flow_field):
+    rng = np.random.default_rng(8)
+    gaps = rng.choice([0.0, 1.0, 7.0, 120.0, 999.0, 2500.0, 40000.0], size=500)
+    pos = np.cumsum(gaps) + 3.0
+    G = (rng.random((6, 500)) < 0.25).astype(np.uint8)
+    pairs = [(i, j) for i in range(6) for j in range(i)]
+    for Ne, mu, rho in ((1e4, 1.25e-8, 1e-8), (2e4, 2e-8, 5e-9), (5e3, 1e-8, 3e-8)):
+        got = G200.gamma_smc_flow_fb(G, pos, pairs, Ne, mu, rho, flow_field)
+        want = oracle.flow_fb(G, pos, pairs, Ne, mu, rho, flow_field)
+        for k in KEYS:
+            assert _max_rel(got[k], want[k]) <= RTOL, (Ne, k, _max_rel(got[k], want[k]))
+
+
+def test_flow_fb_errors(small_data, flow_field, tmp_path):
+    G, pos = small_data
+    assert G200.gamma_smc_flow_fb(G, pos, [], flow_field_path=flow_field)["mean"].shape == \
+        (G.shape[1], 0)
+    with pytest.raises(ValueError, match="out of range"):
+        G200.gamma_smc_flow_fb(G, pos, [(40, 0)], flow_field_path=flow_field)
+    with pytest.raises(RuntimeError, match="flow field"):
+        G200.gamma_smc_flow_fb(G, pos, [(1, 0)], flow_field_path=str(tmp_path / "missing.txt"))
+
+
+def test_flow_fb_bit_exact_with_reference_gpu_build(small_data, flow_field, ref_core):
+    if ref_core is None:
+        pytest.skip("reference _core not built in oracle/_ref")
+    G, pos = small_data
+    pairs = [(i, j) for i in range(40) for j in range(i)]
+    want = ref_core.gamma_smc_flow_fb(G, pos, pairs, 1e4, 1.25e-8, 1e-8, flow_field, False)
+    got = G200.gamma_smc_flow_fb(G, pos, pairs, 1e4, 1.25e-8, 1e-8, flow_field, False)
+    for k in KEYS:
+        assert np.array_equal(got[k], want[k]), (k, _max_rel(got[k], want[k]))

@@ -17,6 +17,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "fwd.h"
 #include "scan_device.cuh"
 
@@ -102,13 +104,25 @@ __global__ void to_half_kernel(const float* __restrict__ src, __half* __restrict
 
 }  // namespace
 
+// Threads per CTA for one thread per pair: as many as keep every SM busy
+// (warps spread over all SMs before SMs get more of them), 32..128.
+int chain_cta_threads(int64_t n_pairs, int max_threads) {
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int64_t t = n_pairs / std::max(1, 2 * sms);
+  t = (t + 31) / 32 * 32;
+  return (int)std::max<int64_t>(32, std::min<int64_t>(t, max_threads));
+}
+
 cudaError_t launch_fwd_only(const FwdArgs& a, cudaStream_t stream) {
   if (a.n_pairs <= 0 || a.n_sites <= 0) return cudaSuccess;
-  const unsigned grid = (unsigned)((a.n_pairs + 127) / 128);
+  const int threads = chain_cta_threads(a.n_pairs, 128);
+  const unsigned grid = (unsigned)((a.n_pairs + threads - 1) / threads);
   if (a.lower && a.upper)
-    fwd_only_kernel<true><<<grid, 128, 0, stream>>>(a);
+    fwd_only_kernel<true><<<grid, threads, 0, stream>>>(a);
   else
-    fwd_only_kernel<false><<<grid, 128, 0, stream>>>(a);
+    fwd_only_kernel<false><<<grid, threads, 0, stream>>>(a);
   return cudaGetLastError();
 }
 

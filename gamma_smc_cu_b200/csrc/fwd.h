@@ -31,6 +31,9 @@ struct FwdArgs {
 };
 
 cudaError_t launch_fwd_only(const FwdArgs& a, cudaStream_t stream);
+// CTA size for kernels with one serial chain per pair: spread the warps over
+// every SM first (32..max_threads threads).
+int chain_cta_threads(int64_t n_pairs, int max_threads);
 // n floats -> n halves (round to nearest even) on the device.
 cudaError_t launch_to_half(const float* src, void* dst, size_t n, cudaStream_t stream);
 

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "fwd.h"
 #include "scan_device.cuh"
 #include "uncached.h"
 
@@ -180,11 +181,14 @@ __global__ void __launch_bounds__(256) uncached_fb_kernel(const UncachedArgs a) 
 
 cudaError_t launch_uncached_fb(const UncachedArgs& a, cudaStream_t stream) {
   if (a.n_pairs <= 0 || a.n_sites <= 0) return cudaSuccess;
-  const unsigned grid = (unsigned)((a.n_pairs + 255) / 256);
+  // every CTA stages its own grid copy: small pair counts get 32-thread CTAs
+  // on as many SMs as possible rather than a few SMs doing everything
+  const int threads = chain_cta_threads(a.n_pairs, 256);
+  const unsigned grid = (unsigned)((a.n_pairs + threads - 1) / threads);
   if (a.lower && a.upper)
-    uncached_fb_kernel<true><<<grid, 256, 0, stream>>>(a);
+    uncached_fb_kernel<true><<<grid, threads, 0, stream>>>(a);
   else
-    uncached_fb_kernel<false><<<grid, 256, 0, stream>>>(a);
+    uncached_fb_kernel<false><<<grid, threads, 0, stream>>>(a);
   return cudaGetLastError();
 }
 

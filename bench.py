@@ -47,8 +47,9 @@ UNIT = "pair-sites/s"
 BYTES_MEAN_ONLY = 4.25      # 4 B fp32 mean + 2 genotype bits per pair-site
 BYTES_FULL_POSTERIOR = 12.25
 # DRAM bytes (read + write) the scan kernel moves per core pair-site in
-# mean-only mode, from an ncu capture of the chromprof case (profiles/
-# fb_scan_persistent_chromprof.md): 16 B forward-state round trip + 4 B output.
+# mean-only mode, from an ncu capture of the same kernel on 6,144 sites x
+# 63,190 pairs (profiles/fb_scan_persistent_scan_case.md): 16 B forward-state
+# round trip + 4 B output.
 TRAFFIC_PER_PAIR_SITE = 20.0
 
 
@@ -65,6 +66,8 @@ def parse():
     ap.add_argument("--no-full-posterior", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--no-stress", action="store_true",
+                    help="skip the 2,000-haplotype x 1,000,000-pair streamed run")
     ap.add_argument("--plain-jobs", type=int, default=48,
                     help="jobs of the mix timed through the plain per-call path")
     return ap.parse_args()
@@ -312,6 +315,9 @@ def main():
     served = None
     if args.workload == "chrom" and not args.no_served:
         served = run_served(dev)
+    stress = None
+    if args.workload == "chrom" and not args.no_stress and rank == 0:
+        stress = run_stream_stress()
 
     e2e = None
     if not args.no_e2e:
@@ -337,6 +343,7 @@ def main():
             "full_posterior": full,
             "batched": batched,
             "served": served,
+            "stream_stress": stress,
             "clocks": clk.summary(),
             "e2e": e2e,
             "cpu_baseline": cpu,
@@ -597,6 +604,54 @@ def run_served(dev, rates=(10, 100, 1000, 2000), seconds=2.0, burst=300):
                 "plain_pair_sites_per_s": ps / wall}
     ctx.close()
     return out
+
+
+def run_stream_stress(core=8192, flank=2048):
+    """Large-cohort stress: 2,000 haplotypes x 200,000 sites (seeds 7/8),
+    1,000,000 random pairs (seed 9), blockwise mean-only streamed to the host
+    through pinned buffers (2e11 posteriors, 800 GB -- beyond host memory, so
+    the sink checks and drops each unit).  Reports the delivered pair-sites/s
+    (wall clock: context + all units on the host) and the scan kernels' own
+    throughput from CUDA events."""
+    import ctypes
+    from gamma_smc_cu_b200 import _core, _lib, synthetic
+    from gamma_smc_cu_b200.infer import _estimate_scaled_params
+    t0 = time.perf_counter()
+    G, pos = synthetic.cohort("cohort")
+    pairs = synthetic.random_pairs(G.shape[0], 1_000_000, 9)
+    gen_s = time.perf_counter() - t0
+    S, P = G.shape[1], len(pairs)
+    mu, rho = _estimate_scaled_params(G, pos, 1.25e-8, 1e-8, 1e4)
+    L = _lib.load()
+    stats = {"units": 0, "bytes": 0, "bad": 0}
+
+    def sink(s0, s1, p0, p1, outs):
+        m = outs["mean"]
+        stats["units"] += 1
+        stats["bytes"] += m.shape[0] * m.shape[1] * 4
+        probe = m[:: max(1, m.shape[0] // 4), :: max(1, m.shape[1] // 8)]
+        stats["bad"] += int((~np.isfinite(probe) | (probe <= 0)).sum())
+        return False
+
+    t0 = time.perf_counter()
+    ctx = _core.FlowContext(G, pos, 1e4, mu, rho, _core.DEFAULT_FLOW_FIELD, 0)
+    _lib.check(L.gsmc_ctx_timing(ctx.handle, 1))
+    ctx.run_fb_blockwise_stream(pairs, sink, core_block_sites=core, flank_sites=flank)
+    wall = time.perf_counter() - t0
+    kms = ctypes.c_double()
+    launches = ctypes.c_int64()
+    psites = ctypes.c_double()
+    _lib.check(L.gsmc_ctx_timing_read(ctx.handle, ctypes.byref(kms), ctypes.byref(launches),
+                                      ctypes.byref(psites)))
+    ctx.close()
+    total = float(S) * P
+    return {"workload": "cohort 2,000 haps x 200,000 sites x 1,000,000 random pairs, blockwise "
+                        f"core {core} / flank {flank}, mean_only, streamed to a host sink",
+            "pair_sites": total, "seconds": wall, "value": total / wall, "unit": UNIT,
+            "d2h_gb_per_s": stats["bytes"] / wall / 1e9, "units": stats["units"],
+            "bad_samples": stats["bad"], "kernel_seconds": kms.value / 1e3,
+            "kernel_pair_sites_per_s": psites.value / (kms.value / 1e3),
+            "gpu_launches": int(launches.value), "data_generation_seconds": gen_s}
 
 
 def run_e2e(G, pos, pairs, core, flank, steps):

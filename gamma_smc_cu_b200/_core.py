@@ -243,6 +243,43 @@ class FlowContext:
                                        ptr(out.get("upper"), _lib.c_f32p)))
         return out
 
+    def run_fb_blockwise_stream(self, pairs, sink, core_block_sites=8192, flank_sites=2048,
+                                pair_batch_size=-1, mean_only=True, return_posterior=False,
+                                max_chunk_bytes=1 << 30):
+        """Blockwise forward-backward streamed to ``sink`` instead of returned:
+        ``sink(site_begin, site_end, pair_begin, pair_end, outputs)`` is called
+        once per (window, pair chunk) with a dict of [site_end - site_begin,
+        pair_end - pair_begin] float32 views (``mean`` and, as selected,
+        ``lower``/``upper``, ``posterior_alpha``/``posterior_beta``) into pinned
+        staging that is reused after the call -- copy what must outlive it.
+        A sink returning True stops the stream (ValueError).  For results
+        larger than host memory; values equal run_fb_blockwise's."""
+        pi, pj = _split_pairs(pairs)
+        P = len(pi)
+        keys = ["mean"] + (["lower", "upper"] if not mean_only else []) + \
+            (["posterior_alpha", "posterior_beta"] if return_posterior else [])
+        flags = (GSMC_CI if not mean_only else 0) | (GSMC_POSTERIOR if return_posterior else 0)
+        index = {"mean": 0, "lower": 1, "upper": 2, "posterior_alpha": 3, "posterior_beta": 4}
+        errors = []
+
+        def trampoline(user, s0, s1, p0, p1, outs, ld):
+            try:
+                rows, n = s1 - s0, p1 - p0
+                views = {k: np.ctypeslib.as_array(outs[index[k]], shape=(rows * ld,))[:rows * ld]
+                         .reshape(rows, ld)[:, :n] for k in keys}
+                return 1 if sink(int(s0), int(s1), int(p0), int(p1), views) else 0
+            except BaseException as e:  # reported after the stream stops
+                errors.append(e)
+                return 1
+
+        cb = _lib.SINK_FN(trampoline)
+        rc = _lib.load().gsmc_run_fb_blockwise_stream(
+            self._h, ptr(pi, _lib.c_i32p), ptr(pj, _lib.c_i32p), P, int(core_block_sites),
+            int(flank_sites), int(pair_batch_size), flags, cb, None, int(max_chunk_bytes))
+        if errors:
+            raise errors[0]
+        check(rc)
+
     def run_fb_summary(self, pairs, core_block_sites=0, flank_sites=2048, pair_batch_size=-1):
         """Per-site mean / min / max over the pairs of the posterior mean, with
         no [n_sites, n_pairs] output (reference ``run_fb_summary``; the

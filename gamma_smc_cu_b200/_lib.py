@@ -67,6 +67,11 @@ class Job(ctypes.Structure):
     ]
 
 
+# gsmc_sink_fn: (user, site_begin, site_end, pair_begin, pair_end, outputs[5], ld) -> int
+SINK_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+                           ctypes.c_int64, ctypes.c_int64,
+                           ctypes.POINTER(ctypes.POINTER(ctypes.c_float)), ctypes.c_int64)
+
 # name -> (restype, argtypes); mirrors include/gsmc_b200.h
 SIGNATURES = {
     "gsmc_last_error": (ctypes.c_char_p, []),
@@ -109,6 +114,8 @@ SIGNATURES = {
     "gsmc_flow_fb": (c_int, [c_u8p, c_i64, c_i64, c_f64p, c_i32p, c_i32p, c_i64, ctypes.c_double,
                              ctypes.c_double, ctypes.c_double, ctypes.c_char_p, c_int, c_f32p,
                              c_f32p, c_f32p]),
+    "gsmc_run_fb_blockwise_stream": (c_int, [c_vp, c_i32p, c_i32p, c_i64, c_i64, c_i64, c_i64,
+                                             c_int, SINK_FN, c_vp, ctypes.c_uint64]),
     "gsmc_ctx_scratch_bytes": (c_int, [c_vp, c_u64p]),
     "gsmc_ctx_timing": (c_int, [c_vp, c_int]),
     "gsmc_ctx_timing_read": (c_int, [c_vp, ctypes.POINTER(ctypes.c_double), c_i64p,

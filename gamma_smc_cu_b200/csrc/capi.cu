@@ -172,6 +172,10 @@ struct gsmc_ctx {
   size_t stage_bytes = 0;
   void* acc = nullptr;     // summary accumulators: double sum, float min, max, mean per site
   size_t acc_bytes = 0;
+  // streaming: pinned host halves the sink reads, and the copy stream
+  float* pinned = nullptr;
+  size_t pinned_bytes = 0;
+  cudaStream_t copy_stream = nullptr;
   std::vector<double> positions;  // host copy, for the forward-only gap codes
   FwdCode* fwd_code = nullptr;    // forward-only gap codes, built on first use
   unsigned char* tasks[2] = {nullptr, nullptr};  // task lists of alternating launches
@@ -616,6 +620,11 @@ int gsmc_ctx_destroy(gsmc_ctx* ctx) {
   cudaFree(ctx->pairs);
   cudaFree(ctx->stage);
   cudaFree(ctx->acc);
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  if (ctx->copy_stream) {
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamDestroy(ctx->copy_stream);
+  }
   cudaFree(ctx->fwd_code);
   for (int i = 0; i < 2; ++i) {
     cudaFree(ctx->tasks[i]);
@@ -905,6 +914,133 @@ int gsmc_run_fwd(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j, in
   if (e != cudaSuccess)
     return fail(GSMC_E_CUDA, "CUDA error: %s (device to host copy)", cudaGetErrorString((cudaError_t)e));
   return GSMC_OK;
+}
+
+int gsmc_run_fb_blockwise_stream(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j,
+                                 int64_t n_pairs, int64_t core_block_sites, int64_t flank_sites,
+                                 int64_t pair_batch_size, int flags, gsmc_sink_fn sink,
+                                 void* user, uint64_t max_chunk_bytes) {
+  if (int rc = check_ctx(ctx)) return rc;
+  if (core_block_sites <= 0) return fail(GSMC_E_INVALID, "core_block_sites must be positive.");
+  if (flank_sites < 0) return fail(GSMC_E_INVALID, "flank_sites must be non-negative.");
+  if (pair_batch_size == 0 || pair_batch_size < -1)
+    return fail(GSMC_E_INVALID, "pair_batch_size must be positive or -1 for auto.");
+  if (n_pairs < 0) return fail(GSMC_E_INVALID, "negative pair count");
+  if (!sink) return fail(GSMC_E_INVALID, "null sink");
+  const int64_t S = ctx->n_sites;
+  if (n_pairs == 0 || S == 0) return GSMC_OK;
+  if (!pair_i || !pair_j) return fail(GSMC_E_INVALID, "null pair arrays");
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  int rc = upload_pairs(ctx, pair_i, pair_j, n_pairs);
+  if (rc) return rc;
+  const std::vector<Block> blocks = make_windows(S, core_block_sites, flank_sites);
+  const int64_t core = max_core(blocks);
+  const int nout = n_outputs(flags);
+  const int tile = scan_tile_pairs(ctx->shape);
+  const int tiles_per_cta = scan_tiles_per_cta(ctx->shape);
+  // a unit is one window x one pair chunk; its outputs fill one stage half
+  const uint64_t unit_cap = max_chunk_bytes ? max_chunk_bytes : (uint64_t)1 << 30;
+  int64_t chunk = std::max<int64_t>(
+      tile, (int64_t)(unit_cap / ((uint64_t)core * nout * sizeof(float))) / tile * tile);
+  if (pair_batch_size > 0) chunk = std::max<int64_t>(1, std::min(chunk, pair_batch_size));
+  chunk = std::min(chunk, n_pairs);
+  const size_t half = (size_t)core * chunk * nout;  // floats
+  rc = ensure_buffer(&ctx->stage, &ctx->stage_bytes, 2 * half * sizeof(float));
+  if (rc) return rc;
+  if (ctx->pinned_bytes < 2 * half * sizeof(float)) {
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    ctx->pinned = nullptr;
+    ctx->pinned_bytes = 0;
+    if (cudaHostAlloc(&ctx->pinned, 2 * half * sizeof(float), cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(GSMC_E_NOMEM, "cudaHostAlloc of %zu bytes of pinned staging failed",
+                  2 * half * sizeof(float));
+    }
+    ctx->pinned_bytes = 2 * half * sizeof(float);
+  }
+  if (!ctx->copy_stream) CUDA_TRY(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+  const int busy = (int)std::min<int64_t>(resident_ctas(ctx->shape),
+                                          ceil_div(ceil_div(chunk, tile), tiles_per_cta));
+  const size_t budget = (size_t)(0.8 * (double)free_device_bytes()) + ctx->pool_bytes;
+  int grid = 0;
+  rc = size_pool(ctx, core, busy, budget, &grid);
+  if (rc) return rc;
+  struct Events {
+    cudaEvent_t computed[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
+    ~Events() {
+      for (int i = 0; i < 2; ++i) {
+        if (computed[i]) cudaEventDestroy(computed[i]);
+        if (copied[i]) cudaEventDestroy(copied[i]);
+      }
+    }
+  } ev;
+  for (int i = 0; i < 2; ++i) {
+    CUDA_TRY(cudaEventCreateWithFlags(&ev.computed[i], cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&ev.copied[i], cudaEventDisableTiming));
+  }
+  const int32_t* d_pi = ctx->pairs;
+  const int32_t* d_pj = ctx->pairs + ctx->pairs_cap;
+  const int selected[5] = {1, (flags & GSMC_CI) ? 1 : 0, (flags & GSMC_CI) ? 1 : 0,
+                           (flags & GSMC_POSTERIOR) ? 1 : 0, (flags & GSMC_POSTERIOR) ? 1 : 0};
+  struct Unit {
+    int64_t b, off, n;
+  };
+  std::vector<Unit> units;
+  for (size_t b = 0; b < blocks.size(); ++b)
+    for (int64_t off = 0; off < n_pairs; off += chunk)
+      units.push_back({(int64_t)b, off, std::min(chunk, n_pairs - off)});
+  // hand unit u (already copied into pinned half u & 1) to the sink
+  auto deliver = [&](size_t u) -> int {
+    const Unit& un = units[u];
+    const Block& blk = blocks[un.b];
+    CUDA_TRY(cudaEventSynchronize(ev.copied[u & 1]));
+    const float* base = ctx->pinned + (u & 1) * half;
+    const float* outs[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    int used = 0;
+    for (int k = 0; k < 5; ++k)
+      if (selected[k]) outs[k] = base + (size_t)(used++) * (blk.ce - blk.cs) * un.n;
+    if (sink(user, blk.cs, blk.ce, un.off, un.off + un.n, outs, un.n) != 0)
+      return fail(GSMC_E_INVALID, "the sink stopped the stream");
+    return GSMC_OK;
+  };
+  for (size_t u = 0; u < units.size(); ++u) {
+    const Unit& un = units[u];
+    const Block& blk = blocks[un.b];
+    const int h = (int)(u & 1);
+    float* st = ctx->stage + (size_t)h * half;
+    const int64_t rows = blk.ce - blk.cs;
+    // the stage half is rewritten only after unit u-2's copy has read it
+    if (u >= 2) CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ev.copied[h], 0));
+    std::vector<Task> tasks;
+    WindowOut wo;
+    int used = 0;
+    for (int k = 0; k < 5; ++k) wo.out[k] = selected[k] ? st + (size_t)(used++) * rows * un.n : nullptr;
+    wo.off = 0;
+    wo.ldo = un.n;
+    wo.row0 = blk.cs;
+    add_window_tasks(blk, d_pi + un.off, d_pj + un.off, un.n, tile, wo, 0, task_flags(flags),
+                     2.0f * ctx->ne, &tasks);
+    rc = launch_tasks(ctx, tasks, h, core, grid, ctx->stream);
+    if (rc) return rc;
+    CUDA_TRY(cudaEventRecord(ev.computed[h], ctx->stream));
+    CUDA_TRY(cudaStreamWaitEvent(ctx->copy_stream, ev.computed[h], 0));
+    CUDA_TRY(cudaMemcpyAsync(ctx->pinned + (size_t)h * half, st,
+                             (size_t)rows * un.n * nout * sizeof(float), cudaMemcpyDeviceToHost,
+                             ctx->copy_stream));
+    CUDA_TRY(cudaEventRecord(ev.copied[h], ctx->copy_stream));
+    // while the GPU computes unit u, the host hands unit u-1 to the sink
+    if (u >= 1) {
+      rc = deliver(u - 1);
+      if (rc) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaStreamSynchronize(ctx->copy_stream);
+        return rc;
+      }
+    }
+  }
+  rc = deliver(units.size() - 1);
+  CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return rc;
 }
 
 int gsmc_run_fb_window(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j,

@@ -137,6 +137,33 @@ int gsmc_run_fb_summary(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pai
 int gsmc_run_fwd(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j, int64_t n_pairs,
                  int flags, float* mean, float* lower, float* upper);
 
+/*
+ * Sink of a streamed blockwise run: called once per (window, pair chunk) with
+ * the core rows [site_begin, site_end) of pairs [pair_begin, pair_end) in
+ * pinned host memory -- outputs[k] (mean, lower, upper, alpha, beta; NULL
+ * where not selected) holds element (s, p) at
+ * outputs[k][(s - site_begin) * ld + (p - pair_begin)] and stays valid only
+ * until the sink returns.  Return 0 to continue, anything else to stop.
+ */
+typedef int (*gsmc_sink_fn)(void* user, int64_t site_begin, int64_t site_end, int64_t pair_begin,
+                            int64_t pair_end, const float* const* outputs, int64_t ld);
+
+/*
+ * Blockwise forward/backward streamed to a host sink instead of one
+ * [n_sites x n_pairs] array, for results larger than host memory: each
+ * (window, pair chunk) unit is computed into a device stage, copied to a
+ * pinned host buffer on a second stream and handed to `sink` on the calling
+ * thread, while the GPU already computes the next unit (double-buffered).
+ * max_chunk_bytes (0 = 1 GiB) bounds one unit's outputs; pair_batch_size
+ * (-1 = auto) caps its pairs.  Values are those of gsmc_run_fb_blockwise.
+ * The sink form of FlowContext::run_fb_blockwise (src/bindings.cpp:
+ * 2991-3345), which fills one pinned host array.
+ */
+int gsmc_run_fb_blockwise_stream(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j,
+                                 int64_t n_pairs, int64_t core_block_sites, int64_t flank_sites,
+                                 int64_t pair_batch_size, int flags, gsmc_sink_fn sink,
+                                 void* user, uint64_t max_chunk_bytes);
+
 /* Number of windows make_block_windows yields for (n_sites, core_block_sites). */
 int gsmc_block_count(int64_t n_sites, int64_t core_block_sites, int64_t* n_blocks);
 

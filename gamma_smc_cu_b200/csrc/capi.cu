@@ -172,6 +172,19 @@ struct gsmc_ctx {
   size_t stage_bytes = 0;
   void* acc = nullptr;     // summary accumulators: double sum, float min, max, mean per site
   size_t acc_bytes = 0;
+  // speculative chunks: boundary records, window descriptors, repair list
+  float2* spec_rec = nullptr;
+  size_t spec_rec_bytes = 0;
+  SpecWindow* spec_win = nullptr;
+  size_t spec_win_bytes = 0;
+  unsigned char* spec_repairs = nullptr;  // [TaskListHead | Task...]
+  size_t spec_repairs_bytes = 0;
+  void* repair_pool = nullptr;            // forward-state slots of the repair launch
+  size_t repair_pool_bytes = 0;
+  bool speculate = true;                  // GSMC_SPECULATE=0 turns chunking off
+  int64_t spec_flank = 2048;              // burn-in sites of a speculative chunk
+  int64_t spec_launches = 0;              // launches that ran speculative chunks
+  int* spec_repaired = nullptr;           // device: (window, pair)s repaired so far
   // streaming: pinned host halves the sink reads, and the copy stream
   float* pinned = nullptr;
   size_t pinned_bytes = 0;
@@ -375,6 +388,126 @@ int size_pool(gsmc_ctx* ctx, int64_t slot_rows, int want, size_t budget, int* gr
   return GSMC_OK;
 }
 
+// ---------------------------------------------------------- speculation --
+// When a launch has fewer (window, pair tile) tasks than the GPU has resident
+// tiles, long windows are cut into chunks that run in parallel: chunk k > 0
+// starts its forward pass spec_flank (2,048) sites before its core, from
+// (0, 0), instead of at the window's start, and chunk k < K-1 starts its
+// backward pass spec_flank sites after its core; chunks have at least
+// 4 x spec_flank core sites.  Each chunk records its boundary
+// states (see Task); a verify kernel compares neighbours bit for bit, and
+// every (window, pair) whose speculative trajectories did not join the exact
+// ones is decoded again whole by a repair launch on the same stream.  The
+// outputs are therefore exactly those of the unchunked window.
+constexpr size_t kRepairPoolBytes = size_t(512) << 20;
+
+struct SpecLaunch {
+  std::vector<SpecWindow> windows;  // windows cut into more than one chunk
+  int64_t n_bnd = 0;                // boundaries over all of them
+  int64_t n_pairs = 0;              // pairs of the launch (record stride)
+  int64_t max_core = 0;             // longest whole core (repair slot rows)
+};
+
+// Chunks per window for a launch of `tasks` tasks on `resident_tiles`
+// tiles: about twice the tiles, chunks of at least kSpecMinCore sites.
+int spec_chunks(const gsmc_ctx* ctx, int64_t tasks, int64_t resident_tiles, int64_t core_len,
+                int flags) {
+  if (!ctx->speculate || (flags & kTaskSummary) || tasks <= 0) return 1;
+  if (tasks >= 2 * resident_tiles) return 1;
+  const int64_t want = ceil_div(2 * resident_tiles, tasks);
+  return (int)std::max<int64_t>(1, std::min<int64_t>(want, core_len / (4 * ctx->spec_flank)));
+}
+
+// Append the tasks of window b for the n pairs at (pi, pj): whole, or in K
+// speculative chunks whose boundary records start at record `sl->n_bnd` of
+// `rec` (already sized).
+void add_spec_window_tasks(const Block& b, int K, int64_t flank, const int32_t* pi,
+                           const int32_t* pj, int64_t n, int tile, const WindowOut& wo,
+                           int64_t col, int flags, float unscale, float2* rec, SpecLaunch* sl,
+                           std::vector<Task>* tasks) {
+  if (K <= 1) {
+    add_window_tasks(b, pi, pj, n, tile, wo, col, flags, unscale, tasks);
+    return;
+  }
+  const int64_t len = b.ce - b.cs;
+  const int64_t bnd0 = sl->n_bnd;
+  for (int k = 0; k < K; ++k) {
+    const int64_t c0 = b.cs + len * k / K, c1 = b.cs + len * (k + 1) / K;
+    const Block cb{c0, c1, k == 0 ? b.ps : std::max(b.ps, c0 - flank),
+                   k == K - 1 ? b.pe : std::min(b.pe, c1 + flank)};
+    const size_t first = tasks->size();
+    add_window_tasks(cb, pi, pj, n, tile, wo, col, flags, unscale, tasks);
+    for (size_t i = first; i < tasks->size(); ++i) {
+      Task& t = (*tasks)[i];
+      const int64_t j = (int64_t)(i - first) * tile;  // the tile's first pair in the launch
+      t.bl = k > 0 ? rec + (bnd0 + k - 1) * 4 * n + j : nullptr;
+      t.br = k < K - 1 ? rec + (bnd0 + k) * 4 * n + j : nullptr;
+      t.bstride = n;
+    }
+  }
+  SpecWindow w;
+  std::memset(&w, 0, sizeof(w));
+  w.first_bnd = (int32_t)bnd0;
+  w.n_bnd = K - 1;
+  std::vector<Task> whole;
+  add_window_tasks(b, pi, pj, 1, 1, wo, col, flags, unscale, &whole);
+  w.repair = whole[0];
+  sl->windows.push_back(w);
+  sl->n_bnd += K - 1;
+  sl->n_pairs = n;
+  sl->max_core = std::max(sl->max_core, len);
+}
+
+// Size the record buffer for `n_bnd` boundaries of n pairs.
+int spec_reserve(gsmc_ctx* ctx, int64_t n_bnd, int64_t n) {
+  if (n_bnd <= 0) return GSMC_OK;
+  return ensure_buffer(&ctx->spec_rec, &ctx->spec_rec_bytes,
+                       (size_t)n_bnd * 4 * n * sizeof(float2));
+}
+
+// After a speculative launch: verify the boundaries, then repair on the
+// same stream.  The repair launch always runs (it ends at once when no pair
+// needs it), so nothing here waits for the device.
+int spec_finish(gsmc_ctx* ctx, const SpecLaunch& sl, cudaStream_t stream) {
+  if (sl.windows.empty()) return GSMC_OK;
+  const int n_win = (int)sl.windows.size();
+  int rc = ensure_buffer(&ctx->spec_win, &ctx->spec_win_bytes, sl.windows.size() * sizeof(SpecWindow));
+  if (rc) return rc;
+  const int64_t max_rep = (int64_t)n_win * sl.n_pairs;
+  rc = ensure_buffer(&ctx->spec_repairs, &ctx->spec_repairs_bytes,
+                     kTaskListHead + (size_t)max_rep * sizeof(Task));
+  if (rc) return rc;
+  const ScanShape rshape{32, 1};
+  const size_t warp_slot = (size_t)sl.max_core * 32 * sizeof(float2);
+  const int64_t rctas = std::max<int64_t>(1, std::min<int64_t>(
+      16, (int64_t)(kRepairPoolBytes / (warp_slot * scan_tiles_per_cta(rshape)))));
+  rc = ensure_buffer(reinterpret_cast<char**>(&ctx->repair_pool), &ctx->repair_pool_bytes,
+                     (size_t)rctas * scan_tiles_per_cta(rshape) * warp_slot);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(ctx->spec_win, sl.windows.data(), sl.windows.size() * sizeof(SpecWindow),
+                           cudaMemcpyHostToDevice, stream));
+  TaskListHead* head = reinterpret_cast<TaskListHead*>(ctx->spec_repairs);
+  Task* repairs = reinterpret_cast<Task*>(ctx->spec_repairs + kTaskListHead);
+  CUDA_TRY(cudaMemsetAsync(head, 0, sizeof(TaskListHead), stream));
+  CUDA_TRY(launch_spec_verify(ctx->spec_rec, sl.n_pairs, ctx->spec_win, n_win, head, repairs,
+                              (int)std::min<int64_t>(max_rep, 0x7fffffff), stream));
+  if (!ctx->spec_repaired) {
+    CUDA_TRY(cudaMalloc(&ctx->spec_repaired, sizeof(int)));
+    CUDA_TRY(cudaMemsetAsync(ctx->spec_repaired, 0, sizeof(int), stream));
+  }
+  CUDA_TRY(launch_add_count(&head->count, ctx->spec_repaired, stream));
+  ScanArgs a;
+  ctx_scan_args(ctx, &a);
+  a.next = &head->next;
+  a.count = &head->count;
+  a.tasks = repairs;
+  a.fwd = static_cast<float2*>(ctx->repair_pool);
+  a.slot_rows = sl.max_core;
+  CUDA_TRY(launch_scan(a, (int)rctas, rshape, stream, false));
+  ctx->spec_launches++;
+  return GSMC_OK;
+}
+
 // All windows x all pairs in one persistent launch, outputs written straight
 // into the caller's device arrays.
 int run_direct(gsmc_ctx* ctx, const int32_t* d_pi, const int32_t* d_pj, int64_t P,
@@ -382,18 +515,34 @@ int run_direct(gsmc_ctx* ctx, const int32_t* d_pi, const int32_t* d_pj, int64_t 
                int64_t col0, cudaStream_t stream) {
   if (P == 0 || blocks.empty()) return GSMC_OK;
   const int tile = scan_tile_pairs(ctx->shape);
+  const int64_t resident_tiles = (int64_t)resident_ctas(ctx->shape) * scan_tiles_per_cta(ctx->shape);
+  const int64_t plain_tasks = (int64_t)blocks.size() * ceil_div(P, tile);
+  std::vector<int> K(blocks.size());
+  int64_t n_bnd = 0;
+  for (size_t i = 0; i < blocks.size(); ++i) {
+    K[i] = spec_chunks(ctx, plain_tasks, resident_tiles, blocks[i].ce - blocks[i].cs, flags);
+    n_bnd += K[i] - 1;
+  }
+  int rc = spec_reserve(ctx, n_bnd, P);
+  if (rc) return rc;
   std::vector<Task> tasks;
-  tasks.reserve(blocks.size() * ceil_div(P, tile));
+  SpecLaunch sl;
   WindowOut wo{{out[0], out[1], out[2], out[3], out[4]}, 0, ld, 0};
-  for (const Block& b : blocks)
-    add_window_tasks(b, d_pi, d_pj, P, tile, wo, col0, task_flags(flags), 2.0f * ctx->ne, &tasks);
+  for (size_t i = 0; i < blocks.size(); ++i)
+    add_spec_window_tasks(blocks[i], K[i], ctx->spec_flank, d_pi, d_pj, P, tile, wo, col0,
+                          task_flags(flags),
+                          2.0f * ctx->ne, ctx->spec_rec, &sl, &tasks);
+  int64_t slot_rows = 0;
+  for (const Task& t : tasks) slot_rows = std::max<int64_t>(slot_rows, t.ce - t.cs);
   const size_t budget = (size_t)(0.8 * (double)free_device_bytes()) + ctx->pool_bytes;
   const int want = (int)std::min<int64_t>(resident_ctas(ctx->shape),
                                           ceil_div((int64_t)tasks.size(), scan_tiles_per_cta(ctx->shape)));
   int grid = 0;
-  int rc = size_pool(ctx, max_core(blocks), want, budget, &grid);
+  rc = size_pool(ctx, slot_rows, want, budget, &grid);
   if (rc) return rc;
-  return launch_tasks(ctx, tasks, 0, max_core(blocks), grid, stream);
+  rc = launch_tasks(ctx, tasks, 0, slot_rows, grid, stream);
+  if (rc) return rc;
+  return spec_finish(ctx, sl, stream);
 }
 
 // Windows x pairs into HOST arrays.  Windows go in groups; each group's
@@ -433,10 +582,22 @@ int run_to_host(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int6
   int rc = ensure_buffer(&ctx->stage, &ctx->stage_bytes, 2 * half * sizeof(float));
   if (rc) return rc;
   const size_t pool_budget = budget > 2 * half * sizeof(float) ? budget - 2 * half * sizeof(float) : slot;
-  // CTAs one launch can keep busy: its (window, pair tile) tasks, at most
-  const int busy = (int)std::min<int64_t>(resident, group * ceil_div(chunk, tile));
+  // speculative chunks per window (the same for every launch): a full
+  // group's plain tasks decide; slots need only the longest chunk core
+  const int ptile = scan_tile_pairs(ctx->shape);
+  const int64_t resident_tiles = (int64_t)resident * scan_tiles_per_cta(ctx->shape);
+  std::vector<int> K(blocks.size());
+  int64_t slot_rows = 0, max_k = 1;
+  for (size_t i = 0; i < blocks.size(); ++i) {
+    const int64_t len = blocks[i].ce - blocks[i].cs;
+    K[i] = spec_chunks(ctx, group * ceil_div(chunk, ptile), resident_tiles, len, flags);
+    slot_rows = std::max(slot_rows, ceil_div(len, K[i]));
+    max_k = std::max<int64_t>(max_k, K[i]);
+  }
+  // CTAs one launch can keep busy: its (chunk, pair tile) tasks, at most
+  const int busy = (int)std::min<int64_t>(resident, group * max_k * ceil_div(chunk, tile));
   int grid = 0;
-  rc = size_pool(ctx, core, busy, pool_budget, &grid);
+  rc = size_pool(ctx, slot_rows, busy, pool_budget, &grid);
   if (rc) return rc;
   for (int i = 0; i < 2; ++i) {
     if (!ctx->stage_free[i]) CUDA_TRY(cudaEventCreateWithFlags(&ctx->stage_free[i], cudaEventDisableTiming));
@@ -457,6 +618,11 @@ int run_to_host(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int6
       if (launch >= 2) CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->stage_free[h], 0));
       // stage layout of this half: [output k][window i][core rows][n pairs]
       std::vector<Task> tasks;
+      int64_t n_bnd = 0;
+      for (int64_t i = 0; i < ng; ++i) n_bnd += K[g0 + i] - 1;
+      rc = spec_reserve(ctx, n_bnd, n);
+      if (rc) return rc;
+      SpecLaunch sl;
       for (int64_t i = 0; i < ng; ++i) {
         const Block& b = blocks[g0 + i];
         WindowOut wo;
@@ -466,10 +632,12 @@ int run_to_host(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int6
         wo.off = i * core * n;
         wo.ldo = n;
         wo.row0 = b.cs;
-        add_window_tasks(b, d_pi + off, d_pj + off, n, scan_tile_pairs(ctx->shape), wo, 0,
-                         task_flags(flags), 2.0f * ctx->ne, &tasks);
+        add_spec_window_tasks(b, K[g0 + i], ctx->spec_flank, d_pi + off, d_pj + off, n, ptile, wo, 0,
+                              task_flags(flags), 2.0f * ctx->ne, ctx->spec_rec, &sl, &tasks);
       }
-      rc = launch_tasks(ctx, tasks, h, core, grid, ctx->stream);
+      rc = launch_tasks(ctx, tasks, h, slot_rows, grid, ctx->stream);
+      if (rc) return rc;
+      rc = spec_finish(ctx, sl, ctx->stream);
       if (rc) return rc;
       CUDA_TRY(cudaEventRecord(ctx->launch_done[h], ctx->stream));
       for (int64_t i = 0; i < ng; ++i) {
@@ -558,6 +726,9 @@ int gsmc_ctx_create(const uint8_t* G, int64_t n_haps, int64_t n_sites, const dou
     const int v = std::atoi(env);
     if (v == 1 || v == 2) ctx->shape.pairs_per_thread = v;
   }
+  if (const char* env = std::getenv("GSMC_SPECULATE")) ctx->speculate = std::atoi(env) != 0;
+  if (const char* env = std::getenv("GSMC_SPEC_FLANK"))
+    ctx->spec_flank = std::max<int64_t>(1, std::atoll(env));
   if (const char* env = std::getenv("GSMC_SCAN_WIDTH")) {
     const int v = std::atoi(env);
     if (v == 32 || v == 128) ctx->shape.width = v;
@@ -620,6 +791,11 @@ int gsmc_ctx_destroy(gsmc_ctx* ctx) {
   cudaFree(ctx->pairs);
   cudaFree(ctx->stage);
   cudaFree(ctx->acc);
+  cudaFree(ctx->spec_rec);
+  cudaFree(ctx->spec_win);
+  cudaFree(ctx->spec_repairs);
+  cudaFree(ctx->repair_pool);
+  cudaFree(ctx->spec_repaired);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   if (ctx->copy_stream) {
     cudaStreamSynchronize(ctx->copy_stream);
@@ -649,6 +825,19 @@ int gsmc_ctx_info(const gsmc_ctx* ctx, int* device, int64_t* n_haps, int64_t* n_
 int gsmc_ctx_scratch_bytes(const gsmc_ctx* ctx, uint64_t* bytes) {
   if (int rc = check_ctx(ctx)) return rc;
   *bytes = ctx->pool_bytes + ctx->stage_bytes + ctx->pairs_cap * 2 * sizeof(int32_t);
+  return GSMC_OK;
+}
+
+int gsmc_ctx_spec_stats(gsmc_ctx* ctx, int64_t* launches, int64_t* repaired) {
+  if (int rc = check_ctx(ctx)) return rc;
+  int r = 0;
+  if (ctx->spec_repaired) {
+    CUDA_TRY(cudaSetDevice(ctx->device));
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    CUDA_TRY(cudaMemcpy(&r, ctx->spec_repaired, sizeof(int), cudaMemcpyDeviceToHost));
+  }
+  if (launches) *launches = ctx->spec_launches;
+  if (repaired) *repaired = r;
   return GSMC_OK;
 }
 

@@ -96,6 +96,8 @@ __global__ void __launch_bounds__(kThreads) fb_scan_noalloc(const NoAllocArgs a)
         task.ldo = a.ldo;
         for (int k = 0; k < 5; ++k) task.out[k] = a.out[k];
         task.unscale = a.unscale;
+        task.bl = task.br = nullptr;  // no speculative chunks here
+        task.bstride = 0;
       }
     }
     __syncthreads();

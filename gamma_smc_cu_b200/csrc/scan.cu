@@ -77,12 +77,41 @@ __global__ void __launch_bounds__(kThreads, NP == 1 ? GSMC_MIN_CTAS : GSMC_MIN_C
       static_assert(sizeof(Task) % 4 == 0, "Task is copied as 32-bit words");
       const int* src = reinterpret_cast<const int*>(a.tasks + id);
       int* dst = reinterpret_cast<int*>(&task[w]);
-      if (lane < (int)(sizeof(Task) / 4)) dst[lane] = src[lane];
+      for (int i = lane; i < (int)(sizeof(Task) / 4); i += 32) dst[i] = src[i];
       __syncwarp();
       scan_task<NP, 32, SUMMARY>(a, task[w], slot);
     }
   }
 }
+
+__device__ __forceinline__ bool same_bits(float2 a, float2 b) {
+  return __float_as_int(a.x) == __float_as_int(b.x) && __float_as_int(a.y) == __float_as_int(b.y);
+}
+
+// Thread (pair p, window w): all boundaries of w must match for p.
+__global__ void spec_verify_kernel(const float2* __restrict__ rec, int64_t n_pairs,
+                                   const SpecWindow* __restrict__ win, TaskListHead* head,
+                                   Task* __restrict__ repairs, int max_repairs) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const SpecWindow& w = win[blockIdx.y];
+  if (p >= n_pairs) return;
+  bool ok = true;
+  for (int b = 0; b < w.n_bnd && ok; ++b) {
+    const float2* r = rec + (int64_t)(w.first_bnd + b) * 4 * n_pairs + p;
+    ok = same_bits(r[0], r[n_pairs]) && same_bits(r[2 * n_pairs], r[3 * n_pairs]);
+  }
+  if (ok) return;
+  const int i = atomicAdd(&head->count, 1);
+  if (i >= max_repairs) return;  // cannot happen: max_repairs covers every (window, pair)
+  Task t = w.repair;
+  t.pi += p;
+  t.pj += p;
+  t.out_off += p;
+  t.pair_count = 1;
+  repairs[i] = t;
+}
+
+__global__ void add_count_kernel(const int* count, int* acc) { *acc += *count; }
 
 // One warp per site row: fold the row's per-warp partials into the site's
 // accumulators.  Lane l sums columns l, l + 32, ... in order, then a fixed
@@ -236,6 +265,20 @@ cudaError_t launch_scan(const ScanArgs& args, int grid, ScanShape shape, cudaStr
     launch_shape<true>(args, grid, shape, stream);
   else
     launch_shape<false>(args, grid, shape, stream);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_spec_verify(const float2* rec, int64_t n_pairs, const SpecWindow* win,
+                               int n_win, TaskListHead* head, Task* repairs, int max_repairs,
+                               cudaStream_t stream) {
+  if (n_pairs <= 0 || n_win <= 0) return cudaSuccess;
+  const dim3 grid((unsigned)((n_pairs + 255) / 256), (unsigned)n_win);
+  spec_verify_kernel<<<grid, 256, 0, stream>>>(rec, n_pairs, win, head, repairs, max_repairs);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_add_count(const int* count, int* acc, cudaStream_t stream) {
+  add_count_kernel<<<1, 1, 0, stream>>>(count, acc);
   return cudaGetLastError();
 }
 

@@ -29,6 +29,18 @@ enum TaskFlags { kTaskCI = 1, kTaskPosterior = 2, kTaskSummary = 4 };
 // pair_count.  Output element (s, pair j of the task) is
 // out[k][out_off + (s - out_row0) * ldo + j] for each selected output k
 // (0 mean, 1 lower, 2 upper, 3 alpha, 4 beta).
+//
+// Speculative chunks: a long window may be cut into chunks whose forward
+// pass starts some sites before the chunk at (0, 0) instead of at the
+// window's start (and whose backward pass starts some sites after it).  Such
+// a task records, for each of its pairs, the states at its chunk boundaries:
+// at the left boundary (bl) the forward state after site cs-1 from its burn-in
+// (kind 1) and the backward state after applying site cs (kind 2); at the
+// right boundary (br) the forward state after site ce-1 (kind 0) and the
+// backward state after applying site ce from its burn-in (kind 3).  Kind k of
+// pair j of the task is at b[k * bstride + j].  A chunk's result is exact when
+// its neighbours' states equal its own bit for bit (the speculative trajectory
+// has joined the exact one); pairs where they do not are recomputed.
 struct Task {
   int32_t ps, cs, ce, pe;
   const int32_t* pi;
@@ -40,7 +52,11 @@ struct Task {
   int64_t out_off;
   int64_t ldo;
   float* out[5];
+  float2* bl;           // left-boundary records, or null
+  float2* br;           // right-boundary records, or null
+  int64_t bstride;
 };
+static_assert(sizeof(Task) == 128, "a warp copies a Task as 32 words");
 
 // Head of a device task list: CTAs take task numbers from `next` (zero when
 // the list is uploaded) until it reaches `count`.  Tasks follow at
@@ -91,6 +107,28 @@ int scan_resident_ctas(ScanShape shape);
 // slot_rows x tile pairs float2.  `summary`: every task is a kTaskSummary task.
 cudaError_t launch_scan(const ScanArgs& args, int grid, ScanShape shape, cudaStream_t stream,
                         bool summary = false);
+
+// A window decoded in speculative chunks: its chunk boundaries are records
+// first_bnd .. first_bnd + n_bnd - 1 of the launch's record buffer, and
+// `repair` is the window decoded whole for the launch's pair 0 (its pi / pj
+// and out_off advance by the pair index, pair_count is set to 1).
+struct SpecWindow {
+  int32_t first_bnd;
+  int32_t n_bnd;
+  int32_t pad[2];
+  Task repair;
+};
+
+// For every (window, pair) of a speculative launch over n_pairs pairs:
+// compare the boundary records (rec: [boundary][4 kinds][n_pairs] float2) bit
+// for bit and append a one-pair repair task to the list at `head` for each
+// pair whose speculative chunks did not join the exact trajectory.
+cudaError_t launch_spec_verify(const float2* rec, int64_t n_pairs, const SpecWindow* win,
+                               int n_win, TaskListHead* head, Task* repairs, int max_repairs,
+                               cudaStream_t stream);
+
+// *acc += *count (one thread), for statistics kept on the device.
+cudaError_t launch_add_count(const int* count, int* acc, cudaStream_t stream);
 
 // Fold per-warp partials (sum, min, max) of a summary launch -- rows x cols,
 // row pitch ld -- into per-site accumulators acc_sum (float64), acc_min,

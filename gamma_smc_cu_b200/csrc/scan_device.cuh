@@ -248,6 +248,16 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     cur = nx;
     nx = nx2;
   }
+  // boundary records of a speculative chunk (see Task); lanes past the task's
+  // last pair write nothing
+  auto record = [&](float2* b, int kind) {
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      const int j = j0 + k * WIDTH;
+      if (j < t.pair_count) b[kind * t.bstride + j] = make_float2(m[k], c[k]);
+    }
+  };
+  if (t.bl) record(t.bl, 1);
   for (; s < ce; ++s) {
     const SiteCode nx2 = code[s + 2];
     fwd_step(s, cur, nx.layer);
@@ -257,6 +267,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     for (int k = 0; k < NP; ++k) __stcs(fp + k * WIDTH, make_float2(m[k], c[k]));
     fp += kRow;
   }
+  if (t.br) record(t.br, 0);
 
   // ---- backward: [pe-1 .. cs]; posterior at core sites ----
 #pragma unroll
@@ -302,6 +313,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     cur = nx;
     nx = nx2;
   }
+  if (t.br) record(t.br, 3);
   // forward-state ring: q[i] holds the state of site s - i
   const float2* fq = slot + (int64_t)(ce - 1 - cs) * kRow + j0;
   float2 q[kFwdPrefetch][NP];
@@ -375,6 +387,14 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     if (more) bwd_finish(sc, fe);
     cur = nx;
     nx = nx2;
+  }
+  if (t.bl) {
+    // the backward state after applying site cs itself, for the left neighbour
+    Fetch fe[NP];
+    const SiteCode scs = code[cs];
+    bwd_fetch(cs, scs, 0, fe);
+    bwd_finish(scs, fe);
+    record(t.bl, 2);
   }
 }
 

@@ -296,6 +296,15 @@ int gsmc_copy_to_host(int64_t n, void* const* dst, const void* const* src,
 int gsmc_ctx_scratch_bytes(const gsmc_ctx* ctx, uint64_t* bytes);
 
 /*
+ * Speculative chunking statistics of a context: launches that cut windows
+ * into parallel chunks (when a call has too few pair tiles to fill the GPU)
+ * and the (window, pair)s whose chunks failed the bitwise boundary check and
+ * were decoded again whole.  Waits for the context's stream.  No reference
+ * counterpart.
+ */
+int gsmc_ctx_spec_stats(gsmc_ctx* ctx, int64_t* launches, int64_t* repaired);
+
+/*
  * Kernel timing for measurement: while enabled, every scan launch of this
  * context is bracketed by CUDA events on the stream it is launched on.
  * gsmc_ctx_timing_read synchronises those events and returns the summed

@@ -505,6 +505,7 @@ int spec_finish(gsmc_ctx* ctx, const SpecLaunch& sl, cudaStream_t stream) {
   a.slot_rows = sl.max_core;
   CUDA_TRY(launch_scan(a, (int)rctas, rshape, stream, false));
   ctx->spec_launches++;
+  ctx->launches += 3;  // verify, count fold, repair scan
   return GSMC_OK;
 }
 

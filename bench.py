@@ -288,6 +288,9 @@ def main():
     _lib.check(L.gsmc_ctx_timing_read(ctx.handle, ctypes.byref(kms), ctypes.byref(launches),
                                       ctypes.byref(psites)))
     _lib.check(L.gsmc_ctx_timing(ctx.handle, 0))
+    width, ppt = ctypes.c_int(), ctypes.c_int()
+    _lib.check(L.gsmc_ctx_scan_shape(ctx.handle, ctypes.byref(width), ctypes.byref(ppt)))
+    kernel_name = f"fb_scan_persistent<{ppt.value}, {width.value}, false>"
     if world > 1:
         t = torch.tensor([t_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -337,7 +340,7 @@ def main():
             "gpu_launches": int(launches.value),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic,
-                         "peak_kind": peak_kind, "kernel": "fb_scan_persistent<1>",
+                         "peak_kind": peak_kind, "kernel": kernel_name,
                          "kernel_ms_per_step": kms.value / args.steps,
                          "bytes_per_pair_site": BYTES_MEAN_ONLY},
             "full_posterior": full,

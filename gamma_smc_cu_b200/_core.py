@@ -339,6 +339,13 @@ class FlowContext:
         result.update(out)
         return result
 
+    def scan_shape(self):
+        """(threads per task, pairs per thread) of the context's latest scan
+        launch; no reference counterpart."""
+        w, k = ctypes.c_int(), ctypes.c_int()
+        check(_lib.load().gsmc_ctx_scan_shape(self._h, ctypes.byref(w), ctypes.byref(k)))
+        return int(w.value), int(k.value)
+
     def table_layer(self, table, layer):
         """Debug: (m_grid, c_grid) [51, 50] of scan table 0..4 at a layer."""
         buf = np.empty(2 * 2550, np.float32)

@@ -161,7 +161,8 @@ struct gsmc_ctx {
   ulonglong2* geno = nullptr;
   SiteCode* code = nullptr;  // site 0 of the code array (kCodePad entries before it)
   TableSet* tables = nullptr;
-  ScanShape shape{128, 1};  // scan launch shape of the context's own calls
+  ScanShape shape{128, 1};  // scan launch shape of the current call (pick_shape)
+  bool shape_fixed = false; // shape set by the environment, not per call
   cudaStream_t stream = nullptr;
   // scratch, grown on demand and kept for the context's lifetime
   void* pool = nullptr;  // forward-state slots of the persistent CTAs
@@ -261,6 +262,17 @@ int resident_ctas(ScanShape shape) {
   int r = std::max(1, scan_resident_ctas(shape));
   if (const char* env = std::getenv("GSMC_MAX_CTAS")) r = std::max(1, std::min(r, std::atoi(env)));
   return r;
+}
+
+// Launch shape of a call over P pairs x n_windows windows: two pairs per
+// thread (two independent lookup chains per thread; ~6% faster on large jobs)
+// when that still gives every resident CTA at least two tasks, else one (twice
+// the tasks, for balance and for speculative chunking of short calls).
+void pick_shape(gsmc_ctx* ctx, int64_t P, int64_t n_windows) {
+  if (ctx->shape_fixed) return;
+  const ScanShape two{scan_threads(), 2};
+  const int64_t tasks = n_windows * ceil_div(P, scan_tile_pairs(two));
+  ctx->shape = tasks >= 2 * (int64_t)resident_ctas(two) ? two : ScanShape{scan_threads(), 1};
 }
 
 // Pair-steps of a task per pair: forward over [ps, ce), backward over [cs, pe).
@@ -515,6 +527,7 @@ int run_direct(gsmc_ctx* ctx, const int32_t* d_pi, const int32_t* d_pj, int64_t 
                const std::vector<Block>& blocks, int flags, float* const out[5], int64_t ld,
                int64_t col0, cudaStream_t stream) {
   if (P == 0 || blocks.empty()) return GSMC_OK;
+  pick_shape(ctx, P, (int64_t)blocks.size());
   const int tile = scan_tile_pairs(ctx->shape);
   const int64_t resident_tiles = (int64_t)resident_ctas(ctx->shape) * scan_tiles_per_cta(ctx->shape);
   const int64_t plain_tasks = (int64_t)blocks.size() * ceil_div(P, tile);
@@ -552,6 +565,7 @@ int run_direct(gsmc_ctx* ctx, const int32_t* d_pi, const int32_t* d_pj, int64_t 
 int run_to_host(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int64_t pair_cap,
                 int flags, float* const host[5], int64_t row0) {
   if (P == 0 || blocks.empty()) return GSMC_OK;
+  pick_shape(ctx, std::min(P, pair_cap), (int64_t)blocks.size());
   HostCopier* copier = HostCopier::for_current_device();
   if (!copier) return fail(GSMC_E_CUDA, "CUDA error: no device for the host copier");
   const int nout = n_outputs(flags);
@@ -726,6 +740,7 @@ int gsmc_ctx_create(const uint8_t* G, int64_t n_haps, int64_t n_sites, const dou
   if (const char* env = std::getenv("GSMC_PAIRS_PER_THREAD")) {
     const int v = std::atoi(env);
     if (v == 1 || v == 2) ctx->shape.pairs_per_thread = v;
+    ctx->shape_fixed = true;
   }
   if (const char* env = std::getenv("GSMC_SPECULATE")) ctx->speculate = std::atoi(env) != 0;
   if (const char* env = std::getenv("GSMC_SPEC_FLANK"))
@@ -733,6 +748,7 @@ int gsmc_ctx_create(const uint8_t* G, int64_t n_haps, int64_t n_sites, const dou
   if (const char* env = std::getenv("GSMC_SCAN_WIDTH")) {
     const int v = std::atoi(env);
     if (v == 32 || v == 128) ctx->shape.width = v;
+    ctx->shape_fixed = true;
   }
   int rc = acquire_tables(ctx->device, flow_field_path, (float)Ne, (float)mu, (float)rho, L,
                           &ctx->tables);
@@ -826,6 +842,13 @@ int gsmc_ctx_info(const gsmc_ctx* ctx, int* device, int64_t* n_haps, int64_t* n_
 int gsmc_ctx_scratch_bytes(const gsmc_ctx* ctx, uint64_t* bytes) {
   if (int rc = check_ctx(ctx)) return rc;
   *bytes = ctx->pool_bytes + ctx->stage_bytes + ctx->pairs_cap * 2 * sizeof(int32_t);
+  return GSMC_OK;
+}
+
+int gsmc_ctx_scan_shape(const gsmc_ctx* ctx, int* width, int* pairs_per_thread) {
+  if (int rc = check_ctx(ctx)) return rc;
+  if (width) *width = ctx->shape.width;
+  if (pairs_per_thread) *pairs_per_thread = ctx->shape.pairs_per_thread;
   return GSMC_OK;
 }
 
@@ -932,6 +955,7 @@ int gsmc_run_fb_summary(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pai
   else
     blocks = make_windows(S, core_block_sites, flank_sites);
   const int64_t core = max_core(blocks);
+  pick_shape(ctx, n_pairs, (int64_t)blocks.size());
   const int tile = scan_tile_pairs(ctx->shape);
   const int warps = ctx->shape.width / 32;  // partial columns per pair tile
   const int resident = resident_ctas(ctx->shape);
@@ -1126,6 +1150,7 @@ int gsmc_run_fb_blockwise_stream(gsmc_ctx* ctx, const int32_t* pair_i, const int
   const std::vector<Block> blocks = make_windows(S, core_block_sites, flank_sites);
   const int64_t core = max_core(blocks);
   const int nout = n_outputs(flags);
+  pick_shape(ctx, n_pairs, (int64_t)blocks.size());
   const int tile = scan_tile_pairs(ctx->shape);
   const int tiles_per_cta = scan_tiles_per_cta(ctx->shape);
   // a unit is one window x one pair chunk; its outputs fill one stage half

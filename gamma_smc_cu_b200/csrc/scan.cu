@@ -29,11 +29,13 @@ namespace {
 
 // Persistent scan: each CTA takes tasks from a global counter until none are
 // left; its forward-state slot is reused task after task.
-// Resident CTAs per SM the register budget is fitted to (128 threads each):
-// 6 leaves the single-pair kernel ~80 registers and no spills, which measured
-// faster than 8 CTAs with spills.
+// Resident CTAs per SM the register budget is fitted to (128 threads each).
+// The single-pair scan is bound by the latency of its lookup chain, so warps
+// per SM matter: 9 CTAs (56 registers, 36 warps, no spill) measured faster
+// than 7 (72 registers) and 8 (64), level with 10 (48, a few spilled bytes)
+// and ahead of 12 (40, spilling).
 #ifndef GSMC_MIN_CTAS
-#define GSMC_MIN_CTAS 6
+#define GSMC_MIN_CTAS 9
 #endif
 
 template <int NP, int WIDTH, bool SUMMARY>

@@ -139,10 +139,11 @@ __device__ __forceinline__ void combine_store(const Task& t, int64_t o, float2 f
 }
 
 // Forward states are read back this many sites ahead of their use so the
-// DRAM latency of that stream is hidden behind the scan's own lookups.  They
+// DRAM latency of that stream is hidden behind the scan's own lookups (two
+// sites of lookups cover it; a deeper ring costs registers and occupancy).  They
 // and the outputs are single-use streams: stored with evict-first (.cs) and
 // read with last-use (.lu) hints so they do not displace table patches.
-constexpr int kFwdPrefetch = 4;
+constexpr int kFwdPrefetch = 2;
 constexpr int kThreads = 128;
 
 // One task: this thread's NP pairs over the task's padded window.  WIDTH
@@ -277,7 +278,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     x[k] = (word_at(gi[k], nh, pe - 1) ^ word_at(gj[k], nh, pe - 1)) << (63 - ((pe - 1) & 63));
   }
   // Backward step at site s: the het/hom site table first, then any full
-  // 1000-bp chunks; split so the combine can run between fetch and finish.
+  // 1000-bp chunks.
   auto bwd_fetch = [&](int s, SiteCode sc, int next_layer, Fetch* f) {
     if ((s & 63) == 63 && s != pe - 1) {
 #pragma unroll
@@ -349,9 +350,9 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
       mb[k] = m[k];
       cb[k] = c[k];
     }
-    Fetch fe[NP];
     const bool more = s > cs;
-    if (more) bwd_fetch(s, sc, nx.layer, fe);
+    // The combine runs before the next lookup is issued: holding the patch
+    // registers across it costs more occupancy than the overlap gains.
     if constexpr (summary) {
       // sum / min / max of the posterior means over the warp's live pairs,
       // in a fixed shuffle order; lane 0 stores the warp's partials
@@ -384,7 +385,11 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
         if (live[k]) combine_store(t, o + k * WIDTH, f[k], mb[k], cb[k], ci, post);
     }
     o -= t.ldo;
-    if (more) bwd_finish(sc, fe);
+    if (more) {
+      Fetch fe[NP];
+      bwd_fetch(s, sc, nx.layer, fe);
+      bwd_finish(sc, fe);
+    }
     cur = nx;
     nx = nx2;
   }

@@ -305,6 +305,14 @@ int gsmc_ctx_scratch_bytes(const gsmc_ctx* ctx, uint64_t* bytes);
 int gsmc_ctx_spec_stats(gsmc_ctx* ctx, int64_t* launches, int64_t* repaired);
 
 /*
+ * Launch shape of the context's most recent scan: threads sharing a task (128
+ * = the CTA, 32 = a warp) and pairs per thread (1 or 2).  Calls with enough
+ * pair tiles to give every resident CTA two tasks run two pairs per thread.
+ * No reference counterpart.
+ */
+int gsmc_ctx_scan_shape(const gsmc_ctx* ctx, int* width, int* pairs_per_thread);
+
+/*
  * Kernel timing for measurement: while enabled, every scan launch of this
  * context is bracketed by CUDA events on the stream it is launched on.
  * gsmc_ctx_timing_read synchronises those events and returns the summed

@@ -265,3 +265,24 @@ def test_gpu_calibration_counts_match_host(oracle):
     G = (np.random.default_rng(3).random((7, 333)) < 0.5).astype(np.uint8)  # odd n, ragged S
     assert np.array_equal(_core.diploid_het_counts(G), oracle.diploid_het_counts(G))
     assert _core.diploid_het_counts(np.zeros((6, 0), np.uint8)).tolist() == [0, 0, 0]
+
+
+def test_two_pairs_per_thread_on_large_calls(oracle, flow_field):
+    """A call with enough pair tiles to give every resident CTA two tasks runs
+    two pairs per thread; a small one runs one.  Both stay bit-exact."""
+    pos = synthetic.positions_for(20000, 4.0e6, 71)
+    G = synthetic.haplotypes(64, pos, 72)
+    mu, rho = oracle.estimate_scaled_params(G, pos, 1.25e-8, 1e-8, NE)
+    ctx = _core.FlowContext(G, pos, NE, mu, rho, flow_field, 0)
+    pairs = [tuple(p) for p in synthetic.all_pairs(G.shape[0])]      # 2,016 pairs
+    got = ctx.run_fb_blockwise(pairs, core_block_sites=64, flank_sites=32,
+                               pair_batch_size=len(pairs))           # 313 windows x 8 tiles
+    assert ctx.scan_shape() == (128, 2)
+    want = oracle.run_fb_blockwise(G, pos, pairs, NE, mu, rho, flow_field, 64, 32)
+    np.testing.assert_array_equal(got["mean"], want["mean"])
+    few = pairs[:40]
+    got = ctx.run_fb_blockwise(few, core_block_sites=4096, flank_sites=512,
+                               pair_batch_size=len(few))
+    assert ctx.scan_shape() == (128, 1)
+    want = oracle.run_fb_blockwise(G, pos, few, NE, mu, rho, flow_field, 4096, 512)
+    np.testing.assert_array_equal(got["mean"], want["mean"])

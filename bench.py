@@ -302,6 +302,7 @@ def main():
     sample = out[::max(1, S // 64), ::max(1, P // 64)]
     assert bool(torch.isfinite(sample).all()) and bool((sample > 0).all()), "bad posterior"
     del out
+    ctx.release_scratch()
     torch.cuda.empty_cache()
     batched = None
     if args.workload == "chrom" and not args.no_batched:
@@ -577,7 +578,7 @@ def run_served(dev, rates=(10, 100, 1000, 2000), seconds=2.0, burst=300):
     out = {"workload": "small cohort 40 haps x 2,127 sites (1 Mb); queries: pairs log-uniform "
                        "[1, 8192] clamped to 780, regions log-uniform [1 kb, 5 Mb] clamped to "
                        "1 Mb, 20% full posterior", "rates": {}}
-    with TmrcaServer(ctx, positions=pos, max_inflight=3) as srv:
+    with TmrcaServer(ctx, positions=pos, max_inflight=3, pinned_bytes=2 << 30) as srv:
         warm = synthetic.request_stream(pos, G.shape[0], 50, 0, seed=60)
         _served_latency(srv, warm)
         for r in warm[:10]:

@@ -339,6 +339,12 @@ class FlowContext:
         result.update(out)
         return result
 
+    def release_scratch(self):
+        """Free the device scratch the context keeps between calls (forward-
+        state slots, stages); genotypes and tables stay.  No reference
+        counterpart."""
+        check(_lib.load().gsmc_ctx_release_scratch(self._h))
+
     def scan_shape(self):
         """(threads per task, pairs per thread) of the context's latest scan
         launch; no reference counterpart."""

@@ -74,6 +74,12 @@ class Job:
         return self.rows * self.n_pairs * self.n_outputs
 
     @property
+    def layout_floats(self):
+        """Floats the job's outputs take in a batch buffer (each output
+        region padded to the 64-float alignment of Layout)."""
+        return -(-(self.rows * self.n_pairs) // _ALIGN) * _ALIGN * self.n_outputs
+
+    @property
     def pair_sites(self):
         return self.rows * self.n_pairs
 

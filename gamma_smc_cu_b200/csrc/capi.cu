@@ -831,6 +831,29 @@ int gsmc_ctx_destroy(gsmc_ctx* ctx) {
   return GSMC_OK;
 }
 
+int gsmc_ctx_release_scratch(gsmc_ctx* ctx) {
+  if (int rc = check_ctx(ctx)) return rc;
+  CUDA_TRY(cudaSetDevice(ctx->device));
+  if (ctx->stream) CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (ctx->copy_stream) CUDA_TRY(cudaStreamSynchronize(ctx->copy_stream));
+  auto drop = [](auto** buf, size_t* bytes) {
+    if (*buf) cudaFree(*buf);
+    *buf = nullptr;
+    *bytes = 0;
+  };
+  drop(&ctx->pool, &ctx->pool_bytes);
+  drop(&ctx->stage, &ctx->stage_bytes);
+  drop(&ctx->acc, &ctx->acc_bytes);
+  drop(&ctx->spec_rec, &ctx->spec_rec_bytes);
+  drop(&ctx->spec_win, &ctx->spec_win_bytes);
+  drop(&ctx->spec_repairs, &ctx->spec_repairs_bytes);
+  drop(&ctx->repair_pool, &ctx->repair_pool_bytes);
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  ctx->pinned = nullptr;
+  ctx->pinned_bytes = 0;
+  return GSMC_OK;
+}
+
 int gsmc_ctx_info(const gsmc_ctx* ctx, int* device, int64_t* n_haps, int64_t* n_sites) {
   if (int rc = check_ctx(ctx)) return rc;
   if (device) *device = ctx->device;

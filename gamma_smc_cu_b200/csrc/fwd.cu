@@ -31,8 +31,8 @@ __device__ __forceinline__ void half_patch_lookup(const uint4* __restrict__ laye
   float fc = __fmul_rn(__fsub_rn(c, kCLo), kCInv);
   fm = fmaxf(0.0f, fminf(fm, (float)(kRows - 1)));
   fc = fmaxf(0.0f, fminf(fc, (float)(kCols - 1)));
-  const float rf = floorf(fminf(fm, (float)kPatchRows - 0.5f));
-  const float qf = floorf(fminf(fc, (float)kPatchCols - 0.5f));
+  const float rf = floor_small(fminf(fm, (float)kPatchRows - 0.5f));
+  const float qf = floor_small(fminf(fc, (float)kPatchCols - 0.5f));
   const float wm = __fsub_rn(fm, rf), wc = __fsub_rn(fc, qf);
   const int idx = __float_as_int(__fadd_rn(__fmaf_rn(rf, (float)kPatchCols, qf), 8388608.0f)) -
                   0x4B000000;

@@ -37,9 +37,14 @@ namespace {
 #ifndef GSMC_MIN_CTAS
 #define GSMC_MIN_CTAS 9
 #endif
+// Two pairs per thread: 7 CTAs (72 registers, no spill) measured faster than
+// 6 (76) and 8 (64, spilling).
+#ifndef GSMC_MIN_CTAS_NP2
+#define GSMC_MIN_CTAS_NP2 7
+#endif
 
 template <int NP, int WIDTH, bool SUMMARY>
-__global__ void __launch_bounds__(kThreads, NP == 1 ? GSMC_MIN_CTAS : GSMC_MIN_CTAS / 2)
+__global__ void __launch_bounds__(kThreads, NP == 1 ? GSMC_MIN_CTAS : GSMC_MIN_CTAS_NP2)
     fb_scan_persistent(const ScanArgs a) {
   // The task descriptor lives in shared memory: its fields are uniform across
   // the tile and read only where used, so they cost no registers.  (Plain

@@ -42,6 +42,13 @@ __device__ __forceinline__ void prefetch_patch(const float4* p) {
 #endif
 }
 
+// floor(x) for 0 <= x < 2^23 in two full-rate adds: x + 2^23 lands in
+// [2^23, 2^24), where floats are the integers, and rounding the sum down keeps
+// 2^23 + floor(x) exactly.
+__device__ __forceinline__ float floor_small(float x) {
+  return __fsub_rn(__fadd_rd(x, 8388608.0f), 8388608.0f);
+}
+
 __device__ __forceinline__ Fetch patch_fetch(const float4* __restrict__ layer, float m, float c) {
   float fm = __fmul_rn(__fsub_rn(m, kMLo), kMInv);
   float fc = __fmul_rn(__fsub_rn(c, kCLo), kCInv);
@@ -50,8 +57,8 @@ __device__ __forceinline__ Fetch patch_fetch(const float4* __restrict__ layer, f
   // Lower-left corner: the reference truncates (fm >= 0, so floor) and moves
   // an index that lands on the last row/column down by one.  floor(min(x,
   // last - 0.5)) is both at once, and the weight stays x - corner.
-  const float rf = floorf(fminf(fm, (float)kPatchRows - 0.5f));
-  const float qf = floorf(fminf(fc, (float)kPatchCols - 0.5f));
+  const float rf = floor_small(fminf(fm, (float)kPatchRows - 0.5f));
+  const float qf = floor_small(fminf(fc, (float)kPatchCols - 0.5f));
   Fetch f;
   f.wm = __fsub_rn(fm, rf);
   f.wc = __fsub_rn(fc, qf);

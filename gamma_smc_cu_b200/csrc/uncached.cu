@@ -73,8 +73,8 @@ __device__ __forceinline__ float2 flow_at(const float2* s_flow, float m, float c
   float fc = __fmul_rn(__fsub_rn(c, kCLo), kCInv);
   fm = fmaxf(0.0f, fminf(fm, (float)(kRows - 1)));
   fc = fmaxf(0.0f, fminf(fc, (float)(kCols - 1)));
-  const float rf = floorf(fminf(fm, (float)kPatchRows - 0.5f));
-  const float qf = floorf(fminf(fc, (float)kPatchCols - 0.5f));
+  const float rf = floor_small(fminf(fm, (float)kPatchRows - 0.5f));
+  const float qf = floor_small(fminf(fc, (float)kPatchCols - 0.5f));
   const float wm = __fsub_rn(fm, rf), wc = __fsub_rn(fc, qf);
   const int base = (int)rf * kCols + (int)qf;
   const float2 v00 = s_flow[base], v01 = s_flow[base + 1];

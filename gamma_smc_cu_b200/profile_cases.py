@@ -7,8 +7,10 @@ Each case builds its inputs, runs the kernel once to warm up and then
 126 MB L2 of a B200 (so DRAM counters mean something) while holding at most a
 few GB on the device.  Cases:
 
-* ``scan``      cached FB, chromosome cohort, 6,144 sites x 63,190 pairs,
-                blockwise core 2,048 / flank 1,024, mean-only
+* ``scan``      cached FB, chromosome cohort, 8,192 sites x 63,190 pairs,
+                blockwise core 512 / flank 128 (16 windows x 247 tiles of 256
+                pairs: enough tasks for the two-pairs-per-thread shape the
+                full chromosome job runs), mean-only
 * ``batch``     64 uneven jobs (1-2,000 pairs, 2k-40k-site windows) over a
                 60,000-site slice of the chromosome cohort, one executor launch
                 (32-thread tiles, 4,096-site chunks)
@@ -36,7 +38,7 @@ def _ctx(n_sites):
 def case_scan(repeat):
     import torch
     from . import _lib, synthetic
-    ctx, G, pos = _ctx(6144)
+    ctx, G, pos = _ctx(8192)
     pairs = synthetic.all_pairs(G.shape[0])
     dev = torch.device("cuda", ctx.device_id)
     pi = torch.from_numpy(np.ascontiguousarray(pairs[:, 0])).to(dev)
@@ -45,9 +47,10 @@ def case_scan(repeat):
     L = _lib.load()
     for _ in range(1 + repeat):
         _lib.check(L.gsmc_run_fb_blockwise_device(
-            ctx.handle, pi.data_ptr(), pj.data_ptr(), len(pairs), 2048, 1024, 0,
+            ctx.handle, pi.data_ptr(), pj.data_ptr(), len(pairs), 512, 128, 0,
             out.data_ptr(), None, None, None, None, len(pairs), 0, None))
     torch.cuda.synchronize()
+    print("scan shape", ctx.scan_shape())
 
 
 def case_batch(repeat):

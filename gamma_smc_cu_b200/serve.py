@@ -97,6 +97,11 @@ class PinnedArena:
                 return None
         return np.asarray(_Region(self, off, n))
 
+    def largest_free(self):
+        """Bytes of the largest free block (the biggest alloc that succeeds)."""
+        with self._lock:
+            return max((ln for _, ln in self._free), default=0)
+
     def release(self, off, n):
         with self._lock:
             self.in_use -= n
@@ -209,7 +214,7 @@ class TmrcaServer:
                   return_posterior=return_posterior)
         validate(job, self.ctx.n_haps, self.ctx.n_sites)
         fut = Future()
-        req = _Request(job, fut, time.perf_counter(), job.output_floats * BYTES_PER_FLOAT,
+        req = _Request(job, fut, time.perf_counter(), job.layout_floats * BYTES_PER_FLOAT,
                        _count_tasks([job], self.config))
         with self._cv:
             if self._closing:
@@ -283,8 +288,17 @@ class TmrcaServer:
         slot.bytes = 0
 
     def _admit(self, slot):
-        """Move the waiting queries that fit into a new batch on ``slot``."""
+        """Move the waiting queries that fit into a new batch on ``slot``.
+
+        A batch's results land in one block of the pinned arena, so it takes no
+        more than the largest free block holds: allocating pinned memory
+        outside the arena costs milliseconds to seconds.  A query larger than
+        the free block waits while other batches are in flight (their results
+        return to the arena as clients drop them); with none in flight, or if
+        it exceeds the whole arena, it runs with its own pinned buffer."""
         take, nbytes, ntasks, work = [], 0, 0, 0.0
+        cap = self.arena.largest_free() if self.arena is not None else None
+        in_flight = any(s.batch is not None for s in self.slots)
         with self._cv:
             while self._pending and len(take) < self.max_batch_requests:
                 req = self._pending[0]
@@ -298,9 +312,13 @@ class TmrcaServer:
                     continue
                 if take and (self._in_use + nbytes + req.bytes > self.hbm_budget
                              or ntasks + req.tasks > self.max_tasks
-                             or work + req.job.pair_sites > self.max_batch_pair_sites):
+                             or work + req.job.pair_sites > self.max_batch_pair_sites
+                             or (cap is not None and nbytes + req.bytes > cap)):
                     break
                 if self._in_use + req.bytes > self.hbm_budget:
+                    break
+                if (not take and cap is not None and req.bytes > cap and in_flight
+                        and req.bytes <= self.arena.size):
                     break
                 self._pending.popleft()
                 take.append(req)

@@ -292,6 +292,15 @@ int gsmc_exec_timing_read(gsmc_exec* exec, double* kernel_ms, int64_t* launches,
 int gsmc_copy_to_host(int64_t n, void* const* dst, const void* const* src,
                       const uint64_t* bytes, void* stream);
 
+/*
+ * Frees the context's device scratch (forward-state slots, output stages,
+ * summary accumulators, speculation buffers) and its pinned staging, after
+ * waiting for its streams.  The next call allocates again; genotypes and
+ * tables stay resident.  For callers that share the device with other
+ * allocations between calls.  No reference counterpart.
+ */
+int gsmc_ctx_release_scratch(gsmc_ctx* ctx);
+
 /* Bytes of device scratch the context currently holds (forward-state pool). */
 int gsmc_ctx_scratch_bytes(const gsmc_ctx* ctx, uint64_t* bytes);
 

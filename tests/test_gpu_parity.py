@@ -286,3 +286,23 @@ def test_two_pairs_per_thread_on_large_calls(oracle, flow_field):
     assert ctx.scan_shape() == (128, 1)
     want = oracle.run_fb_blockwise(G, pos, few, NE, mu, rho, flow_field, 4096, 512)
     np.testing.assert_array_equal(got["mean"], want["mean"])
+
+
+def test_release_scratch_then_rerun(small, flow_field):
+    G, pos, mu, rho = small
+    ctx = _core.FlowContext(G, pos, NE, mu, rho, flow_field, 0)
+    pairs = [(i, j) for i in range(30) for j in range(i)]
+    first = ctx.run_fb_blockwise(pairs, core_block_sites=300, flank_sites=100)["mean"]
+    v = ctypes.c_uint64()
+    _lib.check(_lib.load().gsmc_ctx_scratch_bytes(ctx.handle, ctypes.byref(v)))
+    before = v.value
+    ctx.release_scratch()
+    _lib.check(_lib.load().gsmc_ctx_scratch_bytes(ctx.handle, ctypes.byref(v)))
+    pool_free = v.value  # only the pair-index buffer is kept
+    assert pool_free < before
+    again = ctx.run_fb_blockwise(pairs, core_block_sites=300, flank_sites=100)["mean"]
+    np.testing.assert_array_equal(first, again)
+    ctx.release_scratch()
+    ctx.release_scratch()  # idempotent
+    _lib.check(_lib.load().gsmc_ctx_scratch_bytes(ctx.handle, ctypes.byref(v)))
+    assert v.value == pool_free

@@ -236,3 +236,28 @@ def test_results_outlive_arena_pressure(server_factory):
     for i, r in enumerate(res, start=1):
         assert np.array_equal(r["mean"][:, 1], np.arange(400) + 1000.0 * i)
     assert s.stats()["outside_arena"] >= 1
+
+
+def test_batches_fit_the_arena_when_results_are_dropped(server_factory):
+    """A burst larger than the arena is split into batches that each fit its
+    largest free block; with results dropped as they complete nothing is
+    allocated outside the arena."""
+    s, rec = server_factory(max_inflight=2, pinned_bytes=16384)
+    ok, done = [], threading.Event()
+    n = 24
+
+    def check(i):
+        def cb(f):
+            r = f.result()
+            ok.append(bool(np.array_equal(r["mean"][:, 1], np.arange(400) + 1000.0 * i)))
+            if len(ok) == n:
+                done.set()
+        return cb
+
+    for i in range(1, n + 1):
+        s.submit([(i % 20, 0), (i % 20, 1)], 0, 400).add_done_callback(check(i % 20))
+    assert done.wait(timeout=20)
+    assert all(ok)
+    st = s.stats()
+    assert st.get("outside_arena", 0) == 0
+    assert rec.launches >= n * 3200 // 16384

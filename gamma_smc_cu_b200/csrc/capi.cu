@@ -264,15 +264,29 @@ int resident_ctas(ScanShape shape) {
   return r;
 }
 
-// Launch shape of a call over P pairs x n_windows windows: two pairs per
-// thread (two independent lookup chains per thread; ~6% faster on large jobs)
-// when that still gives every resident CTA at least two tasks, else one (twice
-// the tasks, for balance and for speculative chunking of short calls).
-void pick_shape(gsmc_ctx* ctx, int64_t P, int64_t n_windows) {
+int spec_chunks(const gsmc_ctx* ctx, int64_t tasks, int64_t resident_tiles, int64_t core_len,
+                int flags);
+
+// Launch shape of a call over P pairs x `blocks`: two pairs per thread (two
+// independent lookup chains per thread; 6-8% faster) when that still gives
+// every resident CTA two (window, pair tile) tasks, or at least one once
+// the windows are cut into speculative chunks; else one pair per thread (twice
+// the tasks, for calls too small to fill the GPU either way).
+void pick_shape(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int flags) {
   if (ctx->shape_fixed) return;
   const ScanShape two{scan_threads(), 2};
-  const int64_t tasks = n_windows * ceil_div(P, scan_tile_pairs(two));
-  ctx->shape = tasks >= 2 * (int64_t)resident_ctas(two) ? two : ScanShape{scan_threads(), 1};
+  const int64_t tiles = ceil_div(P, scan_tile_pairs(two));
+  const int64_t tasks = (int64_t)blocks.size() * tiles;
+  const int64_t resident = resident_ctas(two);
+  bool use_two = tasks >= 2 * resident;
+  if (!use_two) {
+    int64_t chunked = 0;
+    for (const Block& b : blocks)
+      chunked += tiles * spec_chunks(ctx, tasks, resident * scan_tiles_per_cta(two), b.ce - b.cs,
+                                     flags);
+    use_two = chunked >= resident;
+  }
+  ctx->shape = use_two ? two : ScanShape{scan_threads(), 1};
 }
 
 // Pair-steps of a task per pair: forward over [ps, ce), backward over [cs, pe).
@@ -527,7 +541,7 @@ int run_direct(gsmc_ctx* ctx, const int32_t* d_pi, const int32_t* d_pj, int64_t 
                const std::vector<Block>& blocks, int flags, float* const out[5], int64_t ld,
                int64_t col0, cudaStream_t stream) {
   if (P == 0 || blocks.empty()) return GSMC_OK;
-  pick_shape(ctx, P, (int64_t)blocks.size());
+  pick_shape(ctx, P, blocks, flags);
   const int tile = scan_tile_pairs(ctx->shape);
   const int64_t resident_tiles = (int64_t)resident_ctas(ctx->shape) * scan_tiles_per_cta(ctx->shape);
   const int64_t plain_tasks = (int64_t)blocks.size() * ceil_div(P, tile);
@@ -565,7 +579,7 @@ int run_direct(gsmc_ctx* ctx, const int32_t* d_pi, const int32_t* d_pj, int64_t 
 int run_to_host(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int64_t pair_cap,
                 int flags, float* const host[5], int64_t row0) {
   if (P == 0 || blocks.empty()) return GSMC_OK;
-  pick_shape(ctx, std::min(P, pair_cap), (int64_t)blocks.size());
+  pick_shape(ctx, std::min(P, pair_cap), blocks, flags);
   HostCopier* copier = HostCopier::for_current_device();
   if (!copier) return fail(GSMC_E_CUDA, "CUDA error: no device for the host copier");
   const int nout = n_outputs(flags);
@@ -978,7 +992,7 @@ int gsmc_run_fb_summary(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pai
   else
     blocks = make_windows(S, core_block_sites, flank_sites);
   const int64_t core = max_core(blocks);
-  pick_shape(ctx, n_pairs, (int64_t)blocks.size());
+  pick_shape(ctx, n_pairs, blocks, kTaskSummary);  // summaries are never chunked
   const int tile = scan_tile_pairs(ctx->shape);
   const int warps = ctx->shape.width / 32;  // partial columns per pair tile
   const int resident = resident_ctas(ctx->shape);
@@ -1173,7 +1187,7 @@ int gsmc_run_fb_blockwise_stream(gsmc_ctx* ctx, const int32_t* pair_i, const int
   const std::vector<Block> blocks = make_windows(S, core_block_sites, flank_sites);
   const int64_t core = max_core(blocks);
   const int nout = n_outputs(flags);
-  pick_shape(ctx, n_pairs, (int64_t)blocks.size());
+  pick_shape(ctx, n_pairs, blocks, kTaskSummary);  // this path does not chunk speculatively
   const int tile = scan_tile_pairs(ctx->shape);
   const int tiles_per_cta = scan_tiles_per_cta(ctx->shape);
   // a unit is one window x one pair chunk; its outputs fill one stage half

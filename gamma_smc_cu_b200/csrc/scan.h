@@ -103,7 +103,6 @@ int scan_resident_ctas(ScanShape shape);
 
 // Launch the persistent scan over the task list of args with `grid`
 // CTAs; CTA b's tile t owns forward-state slot b * tiles_per_cta + t of
-// slot_rows x tile pairs float2.
 // slot_rows x tile pairs float2.  `summary`: every task is a kTaskSummary task.
 cudaError_t launch_scan(const ScanArgs& args, int grid, ScanShape shape, cudaStream_t stream,
                         bool summary = false);

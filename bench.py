@@ -309,6 +309,8 @@ def main():
         batched = run_batched(ctx, G, dev, args.plain_jobs)
     ctx.close()
     torch.cuda.empty_cache()
+    if args.workload == "chrom" and not args.no_batched:
+        batched["small_cohort"] = run_batched_small(dev)
     traffic = (TRAFFIC_PER_PAIR_SITE * psites.value / launches.value
                if launches.value and args.workload != "small" else None)
 
@@ -437,17 +439,23 @@ def _max_rel(a, b):
     return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-30))) if a.size else 0.0
 
 
-def run_batched(ctx, G, dev, plain_jobs):
-    """Uneven batch: 512 jobs (seed 5) over the chromosome cohort -- pair
-    count log-uniform in [1, 4096], window log-uniform in [1e3, 2e5] sites --
-    in one persistent launch with the autotuned launch shape and
+BATCH_WORKLOAD = ("512 jobs (seed 5) over the chromosome cohort: pairs log-uniform "
+                  "[1, 4096], windows log-uniform [1e3, 2e5] sites, mean_only")
+
+
+def run_batched(ctx, G, dev, plain_jobs, jobs=None, workload=BATCH_WORKLOAD):
+    """Uneven batch: by default 512 jobs (seed 5) over the chromosome cohort
+    -- pair count log-uniform in [1, 4096], window log-uniform in [1e3, 2e5]
+    sites -- in one persistent launch with the autotuned launch shape and
     sites-per-chunk, against the plain per-call path (one
-    FlowContext.run_fb_window call per job, host outputs)."""
+    FlowContext.run_fb_window call per job, host outputs) on the first
+    ``plain_jobs`` jobs."""
     import torch
     from gamma_smc_cu_b200 import synthetic
     from gamma_smc_cu_b200.batch import DeviceBatch, Executor, Job, Layout, _count_tasks
     from gamma_smc_cu_b200.tune import autotune, executor_kwargs
-    jobs = [Job(**j) for j in synthetic.job_mix(G.shape[0], G.shape[1], 512, seed=5)]
+    if jobs is None:
+        jobs = [Job(**j) for j in synthetic.job_mix(G.shape[0], G.shape[1], 512, seed=5)]
     total = float(sum(j.pair_sites for j in jobs))
     t0 = time.perf_counter()
     tuned = autotune(ctx, jobs, use_cache=False)
@@ -497,9 +505,7 @@ def run_batched(ctx, G, dev, plain_jobs):
     plain_s = time.perf_counter() - t0
     err = max(_max_rel(g["mean"], w["mean"]) for g, w in zip(got, want))
     ex.close()
-    return {"workload": "512 jobs (seed 5) over the chromosome cohort: pairs log-uniform "
-                        "[1, 4096], windows log-uniform [1e3, 2e5] sites, mean_only",
-            "pair_sites": total, "device_ms": dev_ms, "kernel_ms": kms / max(1, reps),
+    return {"workload": workload, "pair_sites": total, "device_ms": dev_ms, "kernel_ms": kms / max(1, reps),
             "value": total / (dev_ms / 1e3), "unit": UNIT, "gpu_launches_per_batch": 1,
             "tuned": {k: tuned[k] for k in ("tile_width", "pairs_per_thread",
                                             "core_block_sites", "flank_sites")},
@@ -509,6 +515,27 @@ def run_batched(ctx, G, dev, plain_jobs):
             "sample_plain_per_call": sample_ps / plain_s,
             "speedup_vs_plain": plain_s / batched_s,
             "max_rel_mean_vs_plain": err}
+
+
+def run_batched_small(dev):
+    """The same 512-job mix (seed 5) over the small cohort (40 haplotypes,
+    2,127 sites over 1 Mb): pair counts log-uniform in [1, 4096] clamped to
+    its 780 pairs, windows log-uniform in [1 kb, 200 kb] of sequence (1-436
+    sites); batched in one launch against all 512 jobs one call each."""
+    from gamma_smc_cu_b200 import _core, synthetic
+    from gamma_smc_cu_b200.batch import Job
+    from gamma_smc_cu_b200.infer import _estimate_scaled_params
+    G, pos = synthetic.cohort("small")
+    mu, rho = _estimate_scaled_params(G, pos, 1.25e-8, 1e-8, 1e4)
+    ctx = _core.FlowContext(G, pos, 1e4, mu, rho, _core.DEFAULT_FLOW_FIELD, 0)
+    jobs = [Job(**j) for j in synthetic.job_mix_bp(pos, G.shape[0], 512, seed=5)]
+    try:
+        return run_batched(ctx, G, dev, len(jobs), jobs=jobs, workload=(
+            "512 jobs (seed 5) over the small cohort (40 haps x 2,127 sites, 1 Mb): pairs "
+            "log-uniform [1, 4096] clamped to 780, windows log-uniform [1 kb, 200 kb] "
+            "(1-436 sites), mean_only"))
+    finally:
+        ctx.close()
 
 
 def _plain_latency(ctx, reqs, pos):

@@ -147,6 +147,28 @@ def job_mix(n_haps, n_sites, n_jobs=512, seed=5, pairs_range=(1, 4096),
     return jobs
 
 
+def job_mix_bp(positions, n_haps, n_jobs=512, seed=5, pairs_range=(1, 4096),
+               window_bp=(1_000, 200_000)):
+    """job_mix with window lengths in base pairs: each window is log-uniform
+    in window_bp at a uniform start and covers the sites inside it (at least
+    one); pair counts as in job_mix, clamped to the cohort's pairs."""
+    rng = np.random.default_rng(seed)
+    positions = np.asarray(positions, np.float64)
+    n_p = _log_uniform_int(rng, pairs_range[0], pairs_range[1], n_jobs)
+    lo, hi = float(positions[0]), float(positions[-1]) + 1.0
+    jobs = []
+    for p in n_p:
+        length = float(min(hi - lo, np.exp(rng.uniform(np.log(window_bp[0]), np.log(window_bp[1])))))
+        a = float(rng.uniform(lo, hi - length)) if hi - length > lo else lo
+        s0 = int(np.searchsorted(positions, a, side="left"))
+        s1 = int(np.searchsorted(positions, a + length, side="left"))
+        s0 = min(s0, len(positions) - 1)
+        s1 = max(s1, s0 + 1)
+        jobs.append({"pairs": _distinct_pairs(rng, n_haps, int(max(1, p))), "site_begin": s0,
+                     "site_end": s1})
+    return jobs
+
+
 def request_stream(positions, n_haps, n_requests, rate, seed=6, pairs_range=(1, 8192),
                    region_bp=(1_000, 5_000_000), posterior_fraction=0.2):
     """Poisson stream of TMRCA queries: arrival times (s) at ``rate`` per

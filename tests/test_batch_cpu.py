@@ -97,3 +97,18 @@ int main(void) {
             T, m = name.split(".")
             cls = _lib.Job if T == "gsmc_job" else _lib.ExecConfig
             assert getattr(cls, m).offset == int(val), name
+
+
+def test_job_mix_bp_windows_cover_their_sequence():
+    from gamma_smc_cu_b200 import synthetic
+    G, pos = synthetic.cohort("small")
+    jobs = synthetic.job_mix_bp(pos, G.shape[0], 512, seed=5)
+    assert len(jobs) == 512
+    S = G.shape[1]
+    for j in jobs:
+        assert 0 <= j["site_begin"] < j["site_end"] <= S
+        assert 1 <= len(j["pairs"]) <= G.shape[0] * (G.shape[0] - 1) // 2
+        assert len({tuple(p) for p in j["pairs"]}) == len(j["pairs"])
+    widths = [j["site_end"] - j["site_begin"] for j in jobs]
+    assert max(widths) < S and min(widths) >= 1   # 200 kb of a 1 Mb sequence at most
+    assert synthetic.job_mix_bp(pos, G.shape[0], 512, seed=5)[7]["site_begin"] == jobs[7]["site_begin"]

@@ -66,6 +66,7 @@ def parse():
     ap.add_argument("--no-full-posterior", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--no-summary", action="store_true")
     ap.add_argument("--no-stress", action="store_true",
                     help="skip the 2,000-haplotype x 1,000,000-pair streamed run")
     ap.add_argument("--plain-jobs", type=int, default=48,
@@ -307,6 +308,9 @@ def main():
     batched = None
     if args.workload == "chrom" and not args.no_batched:
         batched = run_batched(ctx, G, dev, args.plain_jobs)
+    summary = None
+    if args.workload == "chrom" and not args.no_summary:
+        summary = run_summary(ctx, pairs, S)
     ctx.close()
     torch.cuda.empty_cache()
     if args.workload == "chrom" and not args.no_batched:
@@ -347,6 +351,7 @@ def main():
                          "kernel_ms_per_step": kms.value / args.steps,
                          "bytes_per_pair_site": BYTES_MEAN_ONLY},
             "full_posterior": full,
+            "summary": summary,
             "batched": batched,
             "served": served,
             "stream_stress": stress,
@@ -515,6 +520,23 @@ def run_batched(ctx, G, dev, plain_jobs, jobs=None, workload=BATCH_WORKLOAD):
             "sample_plain_per_call": sample_ps / plain_s,
             "speedup_vs_plain": plain_s / batched_s,
             "max_rel_mean_vs_plain": err}
+
+
+def run_summary(ctx, pairs, S, steps=2):
+    """FlowContext.run_fb_summary(pairs) over the whole chromosome job (the
+    reference's default: one full-sequence window), host arrays out: per-site
+    mean / min / max over all 63,190 pairs, wall clock per call."""
+    plist = [tuple(p) for p in pairs.tolist()]
+    r = ctx.run_fb_summary(plist)                      # warm-up
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        r = ctx.run_fb_summary(plist)
+        times.append(time.perf_counter() - t0)
+    t = float(np.mean(times))
+    ok = bool(np.all(r["site_min"] <= r["site_mean"]) and np.all(r["site_mean"] <= r["site_max"]))
+    return {"workload": f"run_fb_summary, full sequence: {S} sites x {len(plist)} pairs",
+            "seconds": t, "value": len(plist) * S / t, "unit": UNIT, "consistent": ok}
 
 
 def run_batched_small(dev):

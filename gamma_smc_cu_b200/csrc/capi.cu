@@ -573,6 +573,16 @@ int run_direct(gsmc_ctx* ctx, const int32_t* d_pi, const int32_t* d_pj, int64_t 
   return spec_finish(ctx, sl, stream);
 }
 
+// Whether a summary over P pairs x `blocks` should go through per-pair means
+// in speculative chunks: its plain tasks (one-pair-per-thread 128-pair tiles)
+// leave resident tiles idle and its longest window can be cut.
+bool summary_by_pairs(const gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks) {
+  const ScanShape one{scan_threads(), 1};
+  const int64_t tasks = (int64_t)blocks.size() * ceil_div(P, scan_tile_pairs(one));
+  const int64_t resident_tiles = (int64_t)resident_ctas(one) * scan_tiles_per_cta(one);
+  return spec_chunks(ctx, tasks, resident_tiles, max_core(blocks), 0) > 1;
+}
+
 // Windows x pairs into HOST arrays.  Windows go in groups; each group's
 // launch writes its core rows into one half of a device stage while the
 // copier streams the previous group's half to the host.
@@ -992,11 +1002,6 @@ int gsmc_run_fb_summary(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pai
   else
     blocks = make_windows(S, core_block_sites, flank_sites);
   const int64_t core = max_core(blocks);
-  pick_shape(ctx, n_pairs, blocks, kTaskSummary);  // summaries are never chunked
-  const int tile = scan_tile_pairs(ctx->shape);
-  const int warps = ctx->shape.width / 32;  // partial columns per pair tile
-  const int resident = resident_ctas(ctx->shape);
-  const int tiles_per_cta = scan_tiles_per_cta(ctx->shape);
   // accumulators: double sum, float min, max, mean per site
   rc = ensure_buffer(reinterpret_cast<char**>(&ctx->acc), &ctx->acc_bytes, (size_t)S * 20);
   if (rc) return rc;
@@ -1004,6 +1009,40 @@ int gsmc_run_fb_summary(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pai
   float* acc_min = reinterpret_cast<float*>(acc_sum + S);
   float* acc_max = acc_min + S;
   float* d_mean = acc_max + S;
+  const int32_t* d_pi = ctx->pairs;
+  const int32_t* d_pj = ctx->pairs + ctx->pairs_cap;
+  if (summary_by_pairs(ctx, n_pairs, blocks)) {
+    // Too few (window, pair tile) tasks to fill the GPU, and a warp's partial
+    // sums cannot be cut into speculative chunks (a repaired pair could not be
+    // taken back out of them): decode per-pair means in exact speculative
+    // chunks into a [sites x pair batch] matrix and fold it per site.
+    const size_t budget = (size_t)(0.7 * (double)free_device_bytes()) + ctx->pool_bytes +
+                          ctx->stage_bytes;
+    int64_t batch = std::max<int64_t>(1, (int64_t)(0.3 * (double)budget / (double)(S * 4)));
+    batch = std::min(batch, n_pairs);
+    if (pair_batch_size > 0) batch = std::min(batch, pair_batch_size);
+    rc = ensure_buffer(&ctx->stage, &ctx->stage_bytes, (size_t)S * batch * sizeof(float));
+    if (rc) return rc;
+    for (int64_t off = 0; off < n_pairs; off += batch) {
+      const int64_t n = std::min(batch, n_pairs - off);
+      float* const out[5] = {ctx->stage, nullptr, nullptr, nullptr, nullptr};
+      rc = run_direct(ctx, d_pi + off, d_pj + off, n, blocks, 0, out, n, 0, ctx->stream);
+      if (rc) return rc;
+      CUDA_TRY(launch_summary_fold(ctx->stage, ctx->stage, ctx->stage, S, n, n, acc_sum, acc_min,
+                                   acc_max, off == 0, ctx->stream));
+    }
+    CUDA_TRY(launch_summary_finish(acc_sum, S, (double)n_pairs, d_mean, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(site_mean, d_mean, S * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(site_min, acc_min, S * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaMemcpyAsync(site_max, acc_max, S * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return GSMC_OK;
+  }
+  pick_shape(ctx, n_pairs, blocks, kTaskSummary);  // summaries are never chunked
+  const int tile = scan_tile_pairs(ctx->shape);
+  const int warps = ctx->shape.width / 32;  // partial columns per pair tile
+  const int resident = resident_ctas(ctx->shape);
+  const int tiles_per_cta = scan_tiles_per_cta(ctx->shape);
   // pair chunk: partials (3 x S x columns floats) within ~40% of the budget
   const size_t budget = (size_t)(0.7 * (double)free_device_bytes()) + ctx->pool_bytes +
                         ctx->stage_bytes;
@@ -1026,8 +1065,6 @@ int gsmc_run_fb_summary(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pai
   int grid = 0;
   rc = size_pool(ctx, core, busy, pool_budget, &grid);
   if (rc) return rc;
-  const int32_t* d_pi = ctx->pairs;
-  const int32_t* d_pj = ctx->pairs + ctx->pairs_cap;
   int which = 0;
   for (int64_t off = 0; off < n_pairs; off += chunk, which ^= 1) {
     const int64_t n = std::min(chunk, n_pairs - off);

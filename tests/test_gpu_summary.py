@@ -96,3 +96,28 @@ def test_summary_matches_reference_gpu_build(small, flow_field, ref_core):
     got = _core.FlowContext(G, pos, NE, mu, rho, flow_field, 0).run_fb_summary(pairs)
     assert want["n_pairs"] == got["n_pairs"]
     assert _max_rel(got["site_mean"], want["site_mean"]) <= 1e-4
+
+
+def test_summary_of_few_pairs_over_long_windows(oracle, flow_field):
+    """600 pairs over a 20,000-site window leave most of the GPU idle as
+    summary tasks, so the per-pair means are decoded in exact speculative
+    chunks and folded per site; same answer as the oracle, any pair batch."""
+    import ctypes
+    from gamma_smc_cu_b200 import _lib
+    G, pos = synthetic.cohort("chrom", n_sites=20000)
+    mu, rho = oracle.estimate_scaled_params(G, pos, 1.25e-8, 1e-8, NE)
+    ctx = _core.FlowContext(G, pos, NE, mu, rho, flow_field, 0)
+    pairs = [tuple(p) for p in synthetic.random_pairs(356, 600, 11)]
+    got = ctx.run_fb_summary(pairs)
+    launches = ctypes.c_int64()
+    _lib.check(_lib.load().gsmc_ctx_spec_stats(ctx.handle, ctypes.byref(launches), None))
+    assert launches.value >= 1            # the speculative per-pair path ran
+    want = oracle.run_fb_summary(G, pos, pairs, NE, mu, rho, flow_field)
+    _check(got, want)
+    full = oracle.run_fb(G, pos, pairs, NE, mu, rho, flow_field, True, False)["mean"]
+    assert np.array_equal(got["site_min"], full.min(axis=1))
+    assert np.array_equal(got["site_max"], full.max(axis=1))
+    batched = ctx.run_fb_summary(pairs, pair_batch_size=250)     # three pair batches
+    assert _max_rel(batched["site_mean"], got["site_mean"]) <= 1e-6
+    assert np.array_equal(batched["site_min"], got["site_min"])
+    assert np.array_equal(batched["site_max"], got["site_max"])

@@ -573,6 +573,17 @@ int run_direct(gsmc_ctx* ctx, const int32_t* d_pi, const int32_t* d_pj, int64_t 
   return spec_finish(ctx, sl, stream);
 }
 
+// Site chunks of a forward-only call over n pairs x S sites: enough (pair,
+// chunk) threads to fill every SM (2,048 threads each), each chunk at least
+// four burn-ins long.
+int fwd_chunks(const gsmc_ctx* ctx, int64_t n, int64_t S) {
+  if (!ctx->speculate || n <= 0) return 1;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  const int64_t want = ceil_div((int64_t)sms * 2048, n);
+  return (int)std::max<int64_t>(1, std::min<int64_t>(want, S / (4 * ctx->spec_flank)));
+}
+
 // Whether a summary over P pairs x `blocks` should go through per-pair means
 // in speculative chunks: its plain tasks (one-pair-per-thread 128-pair tiles)
 // leave resident tiles idle and its longest window can be cut.
@@ -1187,7 +1198,31 @@ int gsmc_run_fwd(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pair_j, in
     a.lower = ci ? ctx->stage + (size_t)S * n : nullptr;
     a.upper = ci ? ctx->stage + (size_t)2 * S * n : nullptr;
     a.ldo = n;
-    if (e == cudaSuccess) e = launch_fwd_only(a, ctx->stream);
+    FwdSpec sp;
+    std::memset(&sp, 0, sizeof(sp));
+    sp.k_chunks = fwd_chunks(ctx, n, S);
+    if (sp.k_chunks > 1) {
+      rc = ensure_buffer(&ctx->spec_rec, &ctx->spec_rec_bytes,
+                         (size_t)(sp.k_chunks - 1) * 2 * n * sizeof(float2));
+      if (!rc)
+        rc = ensure_buffer(&ctx->spec_repairs, &ctx->spec_repairs_bytes, (size_t)(n + 1) * sizeof(int));
+      if (!rc && !ctx->spec_repaired) {
+        CUDA_TRY(cudaMalloc(&ctx->spec_repaired, sizeof(int)));
+        CUDA_TRY(cudaMemsetAsync(ctx->spec_repaired, 0, sizeof(int), ctx->stream));
+      }
+      if (rc) {
+        copier->drain();
+        cudaEventDestroy(done);
+        return rc;
+      }
+      sp.burn_in = (int)std::min<int64_t>(ctx->spec_flank, S);
+      sp.rec = ctx->spec_rec;
+      sp.repair_count = reinterpret_cast<int*>(ctx->spec_repairs);
+      sp.repair_list = sp.repair_count + 1;
+      sp.repaired_total = ctx->spec_repaired;
+      ctx->spec_launches++;
+    }
+    if (e == cudaSuccess) e = launch_fwd_spec(a, sp, ctx->stream);
     if (e == cudaSuccess) e = cudaEventRecord(done, ctx->stream);
     for (int k = 0; k < nout && e == cudaSuccess; ++k)
       e = copier->enqueue(host[k] + off, (size_t)n_pairs * sizeof(float),

@@ -48,21 +48,23 @@ __device__ __forceinline__ void half_patch_lookup(const uint4* __restrict__ laye
                 __fmul_rn(vm, __fmaf_rn(wc, c0.y, __fmul_rn(vc, c0.x))));
 }
 
-// One thread per pair over all sites.
+// Pair p's filtered scan over sites [s0, s1), starting from (m, c) = (0, 0)
+// before site s0, with outputs from site s_out on (row s of the outputs).
+// spec_rec (if set) receives the state after site s_out - 1, end_rec the
+// state after site s1 - 1.
 template <bool CI>
-__global__ void __launch_bounds__(128) fwd_only_kernel(const FwdArgs a) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= a.n_pairs) return;
+__device__ __forceinline__ void fwd_walk(const FwdArgs& a, int p, int s0, int s_out, int s1,
+                                         float2* spec_rec, float2* end_rec) {
   const int hi = a.pi[p], hj = a.pj[p];
   if (hi < 0 || hi >= a.n_haps || hj < 0 || hj >= a.n_haps) return;  // outputs untouched
   const ulonglong2* gi = a.geno + hi;
   const ulonglong2* gj = a.geno + hj;
   const uint4* chunk = a.tab + (size_t)(a.L - 1) * kPatches;
   float m = 0.0f, c = 0.0f;
-  uint64_t x = 0;
-  float* out = a.mean + p;
-  FwdCode nx = a.code[0];
-  for (int s = 0; s < a.n_sites; ++s) {
+  uint64_t x = word_at(gi, a.n_haps, s0) ^ word_at(gj, a.n_haps, s0);
+  float* out = a.mean + (int64_t)s_out * a.ldo + p;
+  FwdCode nx = a.code[s0];
+  for (int s = s0; s < s1; ++s) {
     const FwdCode sc = nx;
     if (s + 1 < a.n_sites) nx = a.code[s + 1];
     if ((s & 63) == 0) x = word_at(gi, a.n_haps, s) ^ word_at(gj, a.n_haps, s);
@@ -80,6 +82,10 @@ __global__ void __launch_bounds__(128) fwd_only_kernel(const FwdArgs a) {
       m = a_log - b_log;
       c = -0.5f * a_log;
     }
+    if (s < s_out) {  // burn-in of a speculative chunk: no output
+      if (s == s_out - 1 && spec_rec) *spec_rec = make_float2(m, c);
+      continue;
+    }
     const float mg = exp2f(m * 3.321928094887362f) * a.two_ne;
     __stcs(out, mg);
     if (CI) {
@@ -94,6 +100,57 @@ __global__ void __launch_bounds__(128) fwd_only_kernel(const FwdArgs a) {
     }
     out += a.ldo;
   }
+  if (end_rec) *end_rec = make_float2(m, c);
+}
+
+// One thread per pair over all sites.
+template <bool CI>
+__global__ void __launch_bounds__(128) fwd_only_kernel(const FwdArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.n_pairs) return;
+  fwd_walk<CI>(a, p, 0, 0, a.n_sites, nullptr, nullptr);
+}
+
+// Speculative site chunks: thread (pair p, chunk k = blockIdx.y) writes sites
+// [c0, c1) after a burn-in from (0, 0) at c0 - burn; records its state after
+// c0 - 1 (speculative) and after c1 - 1 (to check the next chunk against).
+// rec: [boundary][2][n_pairs], kind 0 = end of the left chunk, 1 = the right
+// chunk's burn-in.
+template <bool CI>
+__global__ void __launch_bounds__(128) fwd_chunk_kernel(const FwdArgs a, FwdSpec sp) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.n_pairs) return;
+  const int k = blockIdx.y, K = sp.k_chunks;
+  const int c0 = (int)((int64_t)a.n_sites * k / K), c1 = (int)((int64_t)a.n_sites * (k + 1) / K);
+  const int s0 = k == 0 ? 0 : max(0, c0 - sp.burn_in);
+  float2* spec = k > 0 ? sp.rec + ((int64_t)(k - 1) * 2 + 1) * a.n_pairs + p : nullptr;
+  float2* end = k < K - 1 ? sp.rec + (int64_t)k * 2 * a.n_pairs + p : nullptr;
+  fwd_walk<CI>(a, p, s0, c0, c1, spec, end);
+}
+
+// Pairs whose chunks did not all join the exact trajectory (bitwise) go on
+// the repair list.
+__global__ void fwd_verify_kernel(const FwdArgs a, FwdSpec sp) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.n_pairs) return;
+  for (int b = 0; b + 1 < sp.k_chunks; ++b) {
+    const float2 e = sp.rec[(int64_t)b * 2 * a.n_pairs + p];
+    const float2 q = sp.rec[((int64_t)b * 2 + 1) * a.n_pairs + p];
+    if (__float_as_int(e.x) != __float_as_int(q.x) || __float_as_int(e.y) != __float_as_int(q.y)) {
+      sp.repair_list[atomicAdd(sp.repair_count, 1)] = p;
+      return;
+    }
+  }
+}
+
+// Listed pairs decoded again over all sites; counts them into the total.
+template <bool CI>
+__global__ void __launch_bounds__(128) fwd_repair_kernel(const FwdArgs a, FwdSpec sp) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = *sp.repair_count;
+  if (t == 0 && n > 0) atomicAdd(sp.repaired_total, n);
+  if (t >= n) return;
+  fwd_walk<CI>(a, sp.repair_list[t], 0, 0, a.n_sites, nullptr, nullptr);
 }
 
 // float32 patches -> half patches, round to nearest even (__float2half_rn).
@@ -123,6 +180,27 @@ cudaError_t launch_fwd_only(const FwdArgs& a, cudaStream_t stream) {
     fwd_only_kernel<true><<<grid, threads, 0, stream>>>(a);
   else
     fwd_only_kernel<false><<<grid, threads, 0, stream>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fwd_spec(const FwdArgs& a, const FwdSpec& sp, cudaStream_t stream) {
+  if (a.n_pairs <= 0 || a.n_sites <= 0) return cudaSuccess;
+  if (sp.k_chunks <= 1) return launch_fwd_only(a, stream);
+  const bool ci = a.lower && a.upper;
+  const int threads = chain_cta_threads((int64_t)a.n_pairs * sp.k_chunks, 128);
+  const dim3 grid((unsigned)((a.n_pairs + threads - 1) / threads), (unsigned)sp.k_chunks);
+  cudaError_t e = cudaMemsetAsync(sp.repair_count, 0, sizeof(int), stream);
+  if (e != cudaSuccess) return e;
+  if (ci)
+    fwd_chunk_kernel<true><<<grid, threads, 0, stream>>>(a, sp);
+  else
+    fwd_chunk_kernel<false><<<grid, threads, 0, stream>>>(a, sp);
+  const unsigned pg = (unsigned)((a.n_pairs + 127) / 128);
+  fwd_verify_kernel<<<pg, 128, 0, stream>>>(a, sp);
+  if (ci)
+    fwd_repair_kernel<true><<<pg, 128, 0, stream>>>(a, sp);
+  else
+    fwd_repair_kernel<false><<<pg, 128, 0, stream>>>(a, sp);
   return cudaGetLastError();
 }
 

@@ -30,7 +30,22 @@ struct FwdArgs {
   int64_t ldo;
 };
 
+// Exact speculative site chunks of a forward-only call: chunk k of K covers
+// sites [S k / K, S (k+1) / K) after `burn_in` sites from (0, 0); the state
+// each chunk reaches at its left boundary is checked bitwise against the left
+// chunk's, and pairs with any mismatch are decoded again whole.
+struct FwdSpec {
+  int k_chunks;
+  int burn_in;
+  float2* rec;          // [k_chunks - 1][2][n_pairs]
+  int* repair_list;     // [n_pairs]
+  int* repair_count;    // zeroed by the launch
+  int* repaired_total;  // incremented by the number repaired
+};
+
 cudaError_t launch_fwd_only(const FwdArgs& a, cudaStream_t stream);
+// Chunked launch (one chunk: the plain kernel): chunk kernel, verify, repair.
+cudaError_t launch_fwd_spec(const FwdArgs& a, const FwdSpec& sp, cudaStream_t stream);
 // CTA size for kernels with one serial chain per pair: spread the warps over
 // every SM first (32..max_threads threads).
 int chain_cta_threads(int64_t n_pairs, int max_threads);

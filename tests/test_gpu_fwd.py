@@ -82,3 +82,40 @@ def test_fwd_chromosome_slice(oracle, flow_field):
     sel = np.random.default_rng(0).choice(3000, 40, replace=False)
     want = oracle.run_fwd(G, pos, [tuple(p) for p in pairs[sel]], NE, mu, rho, flow_field)["mean"]
     assert _max_rel(got[:, sel], want) <= RTOL
+
+
+def _spec_stats(ctx):
+    import ctypes
+    from gamma_smc_cu_b200 import _lib
+    la, rep = ctypes.c_int64(), ctypes.c_int64()
+    _lib.check(_lib.load().gsmc_ctx_spec_stats(ctx.handle, ctypes.byref(la), ctypes.byref(rep)))
+    return la.value, rep.value
+
+
+@pytest.mark.parametrize("flank", [None, "4"])
+def test_fwd_speculative_site_chunks_are_exact(oracle, flow_field, ref_core, monkeypatch, flank):
+    """300 pairs over 40,000 sites fill few SMs as one chain per pair, so the
+    sites are cut into chunks with burn-ins whose joins are checked bitwise;
+    the result equals the unchunked kernel's bit for bit, also when a 4-site
+    burn-in makes most pairs fail the check and be decoded again whole."""
+    G, pos = synthetic.cohort("chrom", n_sites=40000)
+    mu, rho = oracle.estimate_scaled_params(G, pos, 1.25e-8, 1e-8, NE)
+    pairs = [tuple(p) for p in synthetic.random_pairs(356, 300, 13)]
+    monkeypatch.setenv("GSMC_SPECULATE", "0")
+    plain = _core.FlowContext(G, pos, NE, mu, rho, flow_field, 0).run_fwd(pairs, mean_only=False)
+    monkeypatch.delenv("GSMC_SPECULATE")
+    if flank:
+        monkeypatch.setenv("GSMC_SPEC_FLANK", flank)
+    ctx = _core.FlowContext(G, pos, NE, mu, rho, flow_field, 0)
+    got = ctx.run_fwd(pairs, mean_only=False)
+    launches, repaired = _spec_stats(ctx)
+    assert launches >= 1
+    if flank:
+        assert repaired > 0
+    for k in ("mean", "lower", "upper"):
+        assert np.array_equal(got[k], plain[k]), k
+    want = oracle.run_fwd(G, pos, pairs, NE, mu, rho, flow_field, mean_only=True)
+    assert _max_rel(got["mean"], want["mean"]) <= RTOL
+    if ref_core is not None and not flank:
+        ref = ref_core.FlowContext(G, pos, NE, mu, rho, flow_field, 0).run_fwd(pairs, True)
+        assert np.array_equal(got["mean"], ref["mean"])

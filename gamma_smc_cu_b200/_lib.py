@@ -118,6 +118,7 @@ SIGNATURES = {
                                              c_int, SINK_FN, c_vp, ctypes.c_uint64]),
     "gsmc_ctx_spec_stats": (c_int, [c_vp, c_i64p, c_i64p]),
     "gsmc_ctx_scan_shape": (c_int, [c_vp, c_i32p, c_i32p]),
+    "gsmc_flow_fb_stats": (c_int, [c_i32p, c_i64p]),
     "gsmc_ctx_release_scratch": (c_int, [c_vp]),
     "gsmc_ctx_scratch_bytes": (c_int, [c_vp, c_u64p]),
     "gsmc_ctx_timing": (c_int, [c_vp, c_int]),

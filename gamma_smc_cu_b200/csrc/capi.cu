@@ -30,6 +30,13 @@ namespace {
 
 thread_local std::string g_last_error;
 
+// Speculative chunking of the calling thread's last gsmc_flow_fb call.
+struct FlowFbStats {
+  int chunks = 1;
+  int64_t repaired = 0;
+};
+thread_local FlowFbStats g_flow_fb_stats;
+
 int fail(int code, const char* fmt, ...) {
   char buf[1024];
   va_list ap;
@@ -903,6 +910,12 @@ int gsmc_ctx_scratch_bytes(const gsmc_ctx* ctx, uint64_t* bytes) {
   return GSMC_OK;
 }
 
+int gsmc_flow_fb_stats(int* chunks, int64_t* repaired) {
+  if (chunks) *chunks = g_flow_fb_stats.chunks;
+  if (repaired) *repaired = g_flow_fb_stats.repaired;
+  return GSMC_OK;
+}
+
 int gsmc_ctx_scan_shape(const gsmc_ctx* ctx, int* width, int* pairs_per_thread) {
   if (int rc = check_ctx(ctx)) return rc;
   if (width) *width = ctx->shape.width;
@@ -1555,6 +1568,8 @@ int gsmc_flow_fb(const uint8_t* G, int64_t n_haps, int64_t n_sites, const double
     float2* fwd = nullptr;
     float* out = nullptr;
     int* error = nullptr;
+    float2* rec = nullptr;  // speculative chunks: boundary records
+    int* rep = nullptr;     // [repaired total | repair count | repair list]
     cudaStream_t st = nullptr;
     cudaEvent_t done = nullptr;
     ~Bufs() {
@@ -1567,6 +1582,8 @@ int gsmc_flow_fb(const uint8_t* G, int64_t n_haps, int64_t n_sites, const double
       cudaFree(fwd);
       cudaFree(out);
       cudaFree(error);
+      cudaFree(rec);
+      cudaFree(rep);
       if (done) cudaEventDestroy(done);
       if (st) cudaStreamDestroy(st);
     }
@@ -1595,6 +1612,28 @@ int gsmc_flow_fb(const uint8_t* G, int64_t n_haps, int64_t n_sites, const double
   CUDA_TRY(cudaMemcpyAsync(b.pairs, pair_i, n_pairs * sizeof(int32_t), cudaMemcpyHostToDevice, b.st));
   CUDA_TRY(cudaMemcpyAsync(b.pairs + n_pairs, pair_j, n_pairs * sizeof(int32_t),
                            cudaMemcpyHostToDevice, b.st));
+  // exact speculative site chunks when the pairs of a chunk cannot fill every
+  // SM (2,048 threads each); chunks of at least four burn-ins
+  bool speculate = true;
+  int64_t burn = 2048;
+  if (const char* env = std::getenv("GSMC_SPECULATE")) speculate = std::atoi(env) != 0;
+  if (const char* env = std::getenv("GSMC_SPEC_FLANK")) burn = std::max<int64_t>(1, std::atoll(env));
+  int sms = 148;
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  auto chunks_for = [&](int64_t n) {
+    if (!speculate) return 1;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div((int64_t)sms * 2048, n),
+                                                       n_sites / (4 * burn)));
+  };
+  const int k_max = chunks_for(std::min(chunk, n_pairs));
+  g_flow_fb_stats = FlowFbStats{};
+  if (k_max > 1) {
+    CUDA_TRY(cudaMalloc(&b.rec, (size_t)(k_max - 1) * 4 * chunk * sizeof(float2)));
+    CUDA_TRY(cudaMalloc(&b.rep, (size_t)(chunk + 2) * sizeof(int)));
+    CUDA_TRY(cudaMemsetAsync(b.rep, 0, sizeof(int), b.st));
+  }
   CUDA_TRY(cudaStreamSynchronize(b.st));  // host sources may go away after this call
   HostCopier* copier = HostCopier::for_current_device();
   if (!copier) return fail(GSMC_E_CUDA, "CUDA error: no device for the host copier");
@@ -1622,7 +1661,18 @@ int gsmc_flow_fb(const uint8_t* G, int64_t n_haps, int64_t n_sites, const double
     a.upper = ci ? b.out + (size_t)2 * n_sites * n : nullptr;
     a.ldo = n;
     a.error = b.error;
-    if (e == cudaSuccess) e = launch_uncached_fb(a, b.st);
+    UncachedSpec sp;
+    std::memset(&sp, 0, sizeof(sp));
+    sp.k_chunks = std::min(k_max, chunks_for(n));
+    if (sp.k_chunks > 1) {
+      sp.burn_in = (int)std::min<int64_t>(burn, n_sites);
+      sp.rec = b.rec;
+      sp.repaired_total = b.rep;
+      sp.repair_count = b.rep + 1;
+      sp.repair_list = b.rep + 2;
+      g_flow_fb_stats.chunks = std::max(g_flow_fb_stats.chunks, sp.k_chunks);
+    }
+    if (e == cudaSuccess) e = launch_uncached_spec(a, sp, b.st);
     if (e == cudaSuccess) e = cudaEventRecord(b.done, b.st);
     for (int k = 0; k < nout && e == cudaSuccess; ++k)
       e = copier->enqueue(host[k] + off, (size_t)n_pairs * sizeof(float),
@@ -1638,6 +1688,11 @@ int gsmc_flow_fb(const uint8_t* G, int64_t n_haps, int64_t n_sites, const double
   int flag = 0;
   CUDA_TRY(cudaMemcpy(&flag, b.error, sizeof(int), cudaMemcpyDeviceToHost));
   if (flag) return fail(GSMC_E_TIMEOUT, "the flow field copy into shared memory did not complete");
+  if (b.rep) {
+    int repaired = 0;
+    CUDA_TRY(cudaMemcpy(&repaired, b.rep, sizeof(int), cudaMemcpyDeviceToHost));
+    g_flow_fb_stats.repaired = repaired;
+  }
   return GSMC_OK;
 }
 

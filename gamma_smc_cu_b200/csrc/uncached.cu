@@ -134,6 +134,57 @@ __device__ __forceinline__ void segment(const float2* s_flow, int seg, float rho
   if (seg > 1) advance(s_flow, rho * (float)(seg - 1), mu * (float)(seg - 1), m, c);
 }
 
+// Pair p over sites: forward from (0, 0) before site s0 through site c1 - 1,
+// states stored for [c0, c1); backward from (0, 0) after site e1 - 1 down
+// through site c0, posteriors written for [c0, c1).  Boundary records (each
+// optional): fspec = forward state after c0 - 1, fend = after c1 - 1;
+// bspec = backward state after applying site c1 (reached from e1),
+// bend = after applying site c0.
+template <bool CI>
+__device__ __forceinline__ void uncached_walk(const UncachedArgs& a, const float2* s_flow, int p,
+                                              int s0, int c0, int c1, int e1, float2* fspec,
+                                              float2* fend, float2* bspec, float2* bend) {
+  const int hi = a.pi[p], hj = a.pj[p];
+  if (hi < 0 || hi >= a.n_haps || hj < 0 || hj >= a.n_haps) return;
+  const ulonglong2* gi = a.geno + hi;
+  const ulonglong2* gj = a.geno + hj;
+  const int64_t P = a.n_pairs;
+  float m = 0.0f, c = 0.0f;
+  uint64_t x = 0;
+  for (int s = s0; s < c1; ++s) {
+    if ((s & 63) == 0 || s == s0) x = word_at(gi, a.n_haps, s) ^ word_at(gj, a.n_haps, s);
+    const bool het = (x >> (s & 63)) & 1ull;
+    segment(s_flow, a.seg[s], a.rho, a.mu, m, c);
+    emit(het, a.mu, m, c);
+    if (s >= c0)
+      __stcs(a.fwd + (int64_t)s * P + p, make_float2(m, c));
+    else if (s == c0 - 1 && fspec)
+      *fspec = make_float2(m, c);
+  }
+  if (fend) *fend = make_float2(m, c);
+  m = 0.0f;
+  c = 0.0f;
+  Task t;  // output addressing for the shared combine
+  t.unscale = a.unscale;
+  t.out[0] = a.mean;
+  t.out[1] = a.lower;
+  t.out[2] = a.upper;
+  t.out[3] = t.out[4] = nullptr;
+  for (int s = e1 - 1; s >= c0; --s) {
+    if (s < c1) {
+      if (s == c1 - 1 && bspec) *bspec = make_float2(m, c);
+      const float2 f = __ldlu(a.fwd + (int64_t)s * P + p);
+      combine_store(t, (int64_t)s * a.ldo + p, f, m, c, CI, false);
+    }
+    if ((s & 63) == 63 || s == e1 - 1) x = word_at(gi, a.n_haps, s) ^ word_at(gj, a.n_haps, s);
+    const bool het = (x >> (s & 63)) & 1ull;
+    emit(het, a.mu, m, c);
+    segment(s_flow, a.seg[s], a.rho, a.mu, m, c);
+  }
+  if (bend) *bend = make_float2(m, c);
+}
+
+// One thread per pair over all sites.
 template <bool CI>
 __global__ void __launch_bounds__(256) uncached_fb_kernel(const UncachedArgs a) {
   __shared__ __align__(16) float2 s_flow[kGridCells];
@@ -144,37 +195,69 @@ __global__ void __launch_bounds__(256) uncached_fb_kernel(const UncachedArgs a) 
   }
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.n_pairs) return;
-  const int hi = a.pi[p], hj = a.pj[p];
-  if (hi < 0 || hi >= a.n_haps || hj < 0 || hj >= a.n_haps) return;
-  const ulonglong2* gi = a.geno + hi;
-  const ulonglong2* gj = a.geno + hj;
-  const int S = a.n_sites;
+  uncached_walk<CI>(a, s_flow, p, 0, 0, a.n_sites, a.n_sites, nullptr, nullptr, nullptr, nullptr);
+}
+
+// Speculative site chunks: thread (pair p, chunk k = blockIdx.y) decodes sites
+// [c0, c1) with `burn_in` sites of burn-in on each inner side and writes the
+// four boundary records rec[boundary][kind][pair] (kind 0 = forward end of the
+// left chunk, 1 = forward burn-in of the right chunk, 2 = backward end of the
+// right chunk, 3 = backward burn-in of the left chunk).
+template <bool CI>
+__global__ void __launch_bounds__(256) uncached_chunk_kernel(const UncachedArgs a, UncachedSpec sp) {
+  __shared__ __align__(16) float2 s_flow[kGridCells];
+  __shared__ __align__(8) uint64_t bar;
+  if (!stage_flow(s_flow, &bar, a.flow)) {
+    if (threadIdx.x == 0) atomicExch(a.error, 1);
+    return;
+  }
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.n_pairs) return;
+  const int k = blockIdx.y, K = sp.k_chunks, S = a.n_sites;
+  const int c0 = (int)((int64_t)S * k / K), c1 = (int)((int64_t)S * (k + 1) / K);
+  const int s0 = k == 0 ? 0 : max(0, c0 - sp.burn_in);
+  const int e1 = k == K - 1 ? S : min(S, c1 + sp.burn_in);
   const int64_t P = a.n_pairs;
-  float m = 0.0f, c = 0.0f;
-  uint64_t x = 0;
-  for (int s = 0; s < S; ++s) {
-    if ((s & 63) == 0) x = word_at(gi, a.n_haps, s) ^ word_at(gj, a.n_haps, s);
-    const bool het = (x >> (s & 63)) & 1ull;
-    segment(s_flow, a.seg[s], a.rho, a.mu, m, c);
-    emit(het, a.mu, m, c);
-    __stcs(a.fwd + (int64_t)s * P + p, make_float2(m, c));
+  float2* left = k > 0 ? sp.rec + (int64_t)(k - 1) * 4 * P + p : nullptr;
+  float2* right = k < K - 1 ? sp.rec + (int64_t)k * 4 * P + p : nullptr;
+  uncached_walk<CI>(a, s_flow, p, s0, c0, c1, e1, left ? left + P : nullptr, right,
+                    right ? right + 3 * P : nullptr, left ? left + 2 * P : nullptr);
+}
+
+__device__ __forceinline__ bool same_state(float2 a, float2 b) {
+  return __float_as_int(a.x) == __float_as_int(b.x) && __float_as_int(a.y) == __float_as_int(b.y);
+}
+
+// Pairs with any boundary whose records differ (bitwise) go on the repair list.
+__global__ void uncached_verify_kernel(const UncachedArgs a, UncachedSpec sp) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.n_pairs) return;
+  const int64_t P = a.n_pairs;
+  for (int b = 0; b + 1 < sp.k_chunks; ++b) {
+    const float2* r = sp.rec + (int64_t)b * 4 * P + p;
+    if (!same_state(r[0], r[P]) || !same_state(r[2 * P], r[3 * P])) {
+      sp.repair_list[atomicAdd(sp.repair_count, 1)] = p;
+      return;
+    }
   }
-  m = 0.0f;
-  c = 0.0f;
-  Task t;  // output addressing for the shared combine
-  t.unscale = a.unscale;
-  t.out[0] = a.mean;
-  t.out[1] = a.lower;
-  t.out[2] = a.upper;
-  t.out[3] = t.out[4] = nullptr;
-  for (int s = S - 1; s >= 0; --s) {
-    const float2 f = __ldlu(a.fwd + (int64_t)s * P + p);
-    combine_store(t, (int64_t)s * a.ldo + p, f, m, c, CI, false);
-    if ((s & 63) == 63 || s == S - 1) x = word_at(gi, a.n_haps, s) ^ word_at(gj, a.n_haps, s);
-    const bool het = (x >> (s & 63)) & 1ull;
-    emit(het, a.mu, m, c);
-    segment(s_flow, a.seg[s], a.rho, a.mu, m, c);
+}
+
+// Listed pairs decoded again over all sites.
+template <bool CI>
+__global__ void __launch_bounds__(256) uncached_repair_kernel(const UncachedArgs a, UncachedSpec sp) {
+  const int n = *sp.repair_count;
+  if ((int)(blockIdx.x * blockDim.x) >= n) return;  // whole CTAs leave before staging
+  __shared__ __align__(16) float2 s_flow[kGridCells];
+  __shared__ __align__(8) uint64_t bar;
+  if (!stage_flow(s_flow, &bar, a.flow)) {
+    if (threadIdx.x == 0) atomicExch(a.error, 1);
+    return;
   }
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) atomicAdd(sp.repaired_total, n);
+  if (t >= n) return;
+  uncached_walk<CI>(a, s_flow, sp.repair_list[t], 0, 0, a.n_sites, a.n_sites, nullptr, nullptr,
+                    nullptr, nullptr);
 }
 
 }  // namespace
@@ -189,6 +272,27 @@ cudaError_t launch_uncached_fb(const UncachedArgs& a, cudaStream_t stream) {
     uncached_fb_kernel<true><<<grid, threads, 0, stream>>>(a);
   else
     uncached_fb_kernel<false><<<grid, threads, 0, stream>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_uncached_spec(const UncachedArgs& a, const UncachedSpec& sp, cudaStream_t stream) {
+  if (a.n_pairs <= 0 || a.n_sites <= 0) return cudaSuccess;
+  if (sp.k_chunks <= 1) return launch_uncached_fb(a, stream);
+  const bool ci = a.lower && a.upper;
+  const int threads = chain_cta_threads((int64_t)a.n_pairs * sp.k_chunks, 256);
+  const dim3 grid((unsigned)((a.n_pairs + threads - 1) / threads), (unsigned)sp.k_chunks);
+  cudaError_t e = cudaMemsetAsync(sp.repair_count, 0, sizeof(int), stream);
+  if (e != cudaSuccess) return e;
+  if (ci)
+    uncached_chunk_kernel<true><<<grid, threads, 0, stream>>>(a, sp);
+  else
+    uncached_chunk_kernel<false><<<grid, threads, 0, stream>>>(a, sp);
+  const unsigned pg = (unsigned)((a.n_pairs + 127) / 128);
+  uncached_verify_kernel<<<pg, 128, 0, stream>>>(a, sp);
+  if (ci)
+    uncached_repair_kernel<true><<<pg, 128, 0, stream>>>(a, sp);
+  else
+    uncached_repair_kernel<false><<<pg, 128, 0, stream>>>(a, sp);
   return cudaGetLastError();
 }
 

@@ -25,6 +25,21 @@ struct UncachedArgs {
   int* error;              // set to 1 when a CTA's flow-field copy did not land
 };
 
+// Exact speculative site chunks (as FwdSpec for the forward-only path): chunk
+// k of K decodes sites [S k / K, S (k+1) / K) with `burn_in` sites of burn-in
+// on its inner sides; the forward and backward states at every chunk boundary
+// are checked bitwise and pairs with any mismatch are decoded again whole.
+struct UncachedSpec {
+  int k_chunks;
+  int burn_in;
+  float2* rec;          // [k_chunks - 1][4][n_pairs]
+  int* repair_list;     // [n_pairs]
+  int* repair_count;    // zeroed by the launch
+  int* repaired_total;  // incremented by the number repaired
+};
+
 cudaError_t launch_uncached_fb(const UncachedArgs& a, cudaStream_t stream);
+// Chunked launch (one chunk: the plain kernel): chunks, verify, repair.
+cudaError_t launch_uncached_spec(const UncachedArgs& a, const UncachedSpec& sp, cudaStream_t stream);
 
 }  // namespace gsmc

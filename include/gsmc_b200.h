@@ -322,6 +322,15 @@ int gsmc_ctx_spec_stats(gsmc_ctx* ctx, int64_t* launches, int64_t* repaired);
 int gsmc_ctx_scan_shape(const gsmc_ctx* ctx, int* width, int* pairs_per_thread);
 
 /*
+ * Speculative chunking of the calling thread's last gsmc_flow_fb call: site
+ * chunks per pair (1 = none; a call whose pairs cannot fill every SM cuts the
+ * sites into chunks with burn-ins, checked bitwise at every boundary) and the
+ * pairs whose check failed and were decoded again whole.  No reference
+ * counterpart.
+ */
+int gsmc_flow_fb_stats(int* chunks, int64_t* repaired);
+
+/*
  * Kernel timing for measurement: while enabled, every scan launch of this
  * context is bracketed by CUDA events on the stream it is launched on.
  * gsmc_ctx_timing_read synchronises those events and returns the summed

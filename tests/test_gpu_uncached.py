@@ -67,3 +67,42 @@ def test_flow_fb_bit_exact_with_reference_gpu_build(small_data, flow_field, ref_
     got = G200.gamma_smc_flow_fb(G, pos, pairs, 1e4, 1.25e-8, 1e-8, flow_field, False)
     for k in KEYS:
         assert np.array_equal(got[k], want[k]), (k, _max_rel(got[k], want[k]))
+
+
+def _flow_fb_stats():
+    import ctypes
+    from gamma_smc_cu_b200 import _lib
+    k, r = ctypes.c_int(), ctypes.c_int64()
+    _lib.check(_lib.load().gsmc_flow_fb_stats(ctypes.byref(k), ctypes.byref(r)))
+    return k.value, r.value
+
+
+@pytest.mark.parametrize("flank", [None, "4"])
+def test_flow_fb_speculative_site_chunks_are_exact(oracle, flow_field, ref_core, monkeypatch,
+                                                   flank):
+    """200 pairs over 20,000 sites are too few chains to fill the SMs, so the
+    sites are cut into chunks whose forward and backward joins are checked
+    bitwise; equal to the unchunked kernel bit for bit, also when a 4-site
+    burn-in sends pairs to be decoded again whole."""
+    G, pos = synthetic.cohort("chrom", n_sites=20000)
+    pairs = [tuple(p) for p in synthetic.random_pairs(356, 200, 17)]
+    monkeypatch.setenv("GSMC_SPECULATE", "0")
+    plain = G200.gamma_smc_flow_fb(G, pos, pairs, Ne=1e4, flow_field_path=flow_field)
+    assert _flow_fb_stats()[0] == 1
+    monkeypatch.delenv("GSMC_SPECULATE")
+    if flank:
+        monkeypatch.setenv("GSMC_SPEC_FLANK", flank)
+    got = G200.gamma_smc_flow_fb(G, pos, pairs, Ne=1e4, flow_field_path=flow_field)
+    chunks, repaired = _flow_fb_stats()
+    assert chunks > 1
+    if flank:
+        assert repaired > 0
+    for k in KEYS:
+        assert np.array_equal(got[k], plain[k]), k
+    if not flank:
+        want = oracle.flow_fb(G, pos, pairs, 1e4, 1.25e-8, 1e-8, flow_field)
+        assert _max_rel(got["mean"], want["mean"]) <= RTOL
+        if ref_core is not None:
+            ref = ref_core.gamma_smc_flow_fb(G, pos, pairs, 1e4, 1.25e-8, 1e-8, flow_field, False)
+            for k in KEYS:
+                assert np.array_equal(got[k], ref[k]), k

@@ -19,6 +19,9 @@ few GB on the device.  Cases:
 * ``fwd``       forward-only posterior, 8,192 pairs x 20,000 sites
 * ``uncached``  uncached flow-field FB, 4,096 pairs x 10,000 sites
 * ``flowgen``   GPU flow-field generation, 51 x 50 cells, constant Ne
+* ``fwd_spec``  forward-only posterior, 2,000 pairs x 400,000 sites (few pairs:
+                the sites run in exact speculative chunks)
+* ``uncached_spec`` uncached flow-field FB, 500 pairs x 200,000 sites (same)
 """
 from __future__ import annotations
 
@@ -104,8 +107,25 @@ def case_flowgen(repeat):
         generate_flow_field(verbose=False)
 
 
+def case_fwd_spec(repeat):
+    from . import synthetic
+    ctx, G, pos = _ctx(400000)
+    pairs = synthetic.random_pairs(G.shape[0], 2000, 4)
+    for _ in range(1 + repeat):
+        ctx.run_fwd(pairs)
+
+
+def case_uncached_spec(repeat):
+    from . import _core, synthetic
+    G, pos = synthetic.cohort("chrom", n_sites=200000)
+    pairs = synthetic.random_pairs(G.shape[0], 500, 4)
+    for _ in range(1 + repeat):
+        _core.gamma_smc_flow_fb(G, pos, pairs, mean_only=True)
+
+
 CASES = {"scan": case_scan, "batch": case_batch, "summary": case_summary, "fwd": case_fwd,
-         "uncached": case_uncached, "flowgen": case_flowgen}
+         "uncached": case_uncached, "flowgen": case_flowgen, "fwd_spec": case_fwd_spec,
+         "uncached_spec": case_uncached_spec}
 
 
 def main():

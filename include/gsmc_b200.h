@@ -67,6 +67,9 @@ int gsmc_get_device(int* device);
  * ensure_flow_field / ensure_cache (src/bindings.cpp:2002-2157) and
  * bitpack_genotypes_gpu (src/kernels/bitpack.cu:32-38).  Tables are owned per
  * parameter set and reference-counted, never freed under a live context.
+ * A context serves one call at a time (its scratch, stream and launch shape
+ * belong to the running call); threads that decode concurrently use one
+ * context each, or executors (gsmc_exec_*) of a shared context.
  */
 int gsmc_ctx_create(const uint8_t* G, int64_t n_haps, int64_t n_sites,
                     const double* positions, double Ne, double mu, double rho,

@@ -30,17 +30,16 @@ namespace {
 // Persistent scan: each CTA takes tasks from a global counter until none are
 // left; its forward-state slot is reused task after task.
 // Resident CTAs per SM the register budget is fitted to (128 threads each).
-// The single-pair scan is bound by the latency of its lookup chain, so warps
-// per SM matter: 9 CTAs (56 registers, 36 warps, no spill) measured faster
-// than 7 (72 registers) and 8 (64), level with 10 (48, a few spilled bytes)
-// and ahead of 12 (40, spilling).
+// The scan is bound by the latency of its lookup chain and by issue, so warps
+// per SM matter.  One pair per thread: 10 CTAs (48 registers with a one-deep
+// forward-state ring, no spill; 9 CTAs at 56 registers ran level, 7-8 slower).
+// Two pairs per thread: 8 CTAs (64 registers, no spill) measured 3% faster
+// than 7 (69-72 registers).
 #ifndef GSMC_MIN_CTAS
-#define GSMC_MIN_CTAS 9
+#define GSMC_MIN_CTAS 10
 #endif
-// Two pairs per thread: 7 CTAs (72 registers, no spill) measured faster than
-// 6 (76) and 8 (64, spilling).
 #ifndef GSMC_MIN_CTAS_NP2
-#define GSMC_MIN_CTAS_NP2 7
+#define GSMC_MIN_CTAS_NP2 8
 #endif
 
 template <int NP, int WIDTH, bool SUMMARY>

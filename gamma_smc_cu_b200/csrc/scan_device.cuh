@@ -146,11 +146,12 @@ __device__ __forceinline__ void combine_store(const Task& t, int64_t o, float2 f
 }
 
 // Forward states are read back this many sites ahead of their use so the
-// DRAM latency of that stream is hidden behind the scan's own lookups (two
-// sites of lookups cover it; a deeper ring costs registers and occupancy).  They
-// and the outputs are single-use streams: stored with evict-first (.cs) and
-// read with last-use (.lu) hints so they do not displace table patches.
-constexpr int kFwdPrefetch = 2;
+// DRAM latency of that stream is hidden behind the scan's own lookups (one
+// site of lookups, combine and the other warps' work covers it; each deeper
+// slot costs registers, and registers cost resident CTAs).  They and the
+// outputs are single-use streams: stored with evict-first (.cs) and read with
+// last-use (.lu) hints so they do not displace table patches.
+constexpr int kFwdPrefetch = 1;
 constexpr int kThreads = 128;
 
 // One task: this thread's NP pairs over the task's padded window.  WIDTH

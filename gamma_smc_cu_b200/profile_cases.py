@@ -11,6 +11,10 @@ few GB on the device.  Cases:
                 blockwise core 512 / flank 128 (16 windows x 247 tiles of 256
                 pairs: enough tasks for the two-pairs-per-thread shape the
                 full chromosome job runs), mean-only
+* ``full``      cached FB with the full posterior (mean + alpha + beta, the
+                output-write-bound mode), chromosome cohort, 4,096 sites x
+                63,190 pairs, blockwise core 256 / flank 64 (16 windows: the
+                two-pairs-per-thread shape)
 * ``batch``     64 uneven jobs (1-2,000 pairs, 2k-40k-site windows) over a
                 60,000-site slice of the chromosome cohort, one executor launch
                 (32-thread tiles, 4,096-site chunks)
@@ -52,6 +56,25 @@ def case_scan(repeat):
         _lib.check(L.gsmc_run_fb_blockwise_device(
             ctx.handle, pi.data_ptr(), pj.data_ptr(), len(pairs), 512, 128, 0,
             out.data_ptr(), None, None, None, None, len(pairs), 0, None))
+    torch.cuda.synchronize()
+    print("scan shape", ctx.scan_shape())
+
+
+def case_full(repeat):
+    import torch
+    from . import _lib, synthetic
+    ctx, G, pos = _ctx(4096)
+    pairs = synthetic.all_pairs(G.shape[0])
+    dev = torch.device("cuda", ctx.device_id)
+    pi = torch.from_numpy(np.ascontiguousarray(pairs[:, 0])).to(dev)
+    pj = torch.from_numpy(np.ascontiguousarray(pairs[:, 1])).to(dev)
+    outs = [torch.empty((G.shape[1], len(pairs)), device=dev) for _ in range(3)]
+    L = _lib.load()
+    for _ in range(1 + repeat):
+        _lib.check(L.gsmc_run_fb_blockwise_device(
+            ctx.handle, pi.data_ptr(), pj.data_ptr(), len(pairs), 256, 64, _lib.GSMC_POSTERIOR,
+            outs[0].data_ptr(), None, None, outs[1].data_ptr(), outs[2].data_ptr(), len(pairs), 0,
+            None))
     torch.cuda.synchronize()
     print("scan shape", ctx.scan_shape())
 
@@ -123,7 +146,7 @@ def case_uncached_spec(repeat):
         _core.gamma_smc_flow_fb(G, pos, pairs, mean_only=True)
 
 
-CASES = {"scan": case_scan, "batch": case_batch, "summary": case_summary, "fwd": case_fwd,
+CASES = {"scan": case_scan, "full": case_full, "batch": case_batch, "summary": case_summary, "fwd": case_fwd,
          "uncached": case_uncached, "flowgen": case_flowgen, "fwd_spec": case_fwd_spec,
          "uncached_spec": case_uncached_spec}
 

@@ -473,7 +473,8 @@ def run_batched(ctx, G, dev, plain_jobs, jobs=None, workload=BATCH_WORKLOAD):
     b.allocate(st)
     with torch.cuda.stream(st):
         b.d_pairs.copy_(b.h_pairs, non_blocking=True)
-    run = lambda: ex.run(b.layout, b.d_pairs.data_ptr(), b.d_out.data_ptr(), st.cuda_stream)
+    run = lambda: ex.run(b.layout, b.d_pairs.data_ptr(), b.d_out.data_ptr(), st.cuda_stream,
+                         flags=b.d_flags.data_ptr())   # chunked jobs checked on the device
     for _ in range(2):
         run()
     st.synchronize()

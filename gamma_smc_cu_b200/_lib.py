@@ -100,6 +100,7 @@ SIGNATURES = {
     "gsmc_exec_destroy": (c_int, [c_vp]),
     "gsmc_exec_info": (c_int, [c_vp, c_intp, c_u64p, c_i64p, c_i64p]),
     "gsmc_exec_run": (c_int, [c_vp, ctypes.POINTER(Job), c_i64, c_vp]),
+    "gsmc_exec_run_checked": (c_int, [c_vp, ctypes.POINTER(Job), c_i64, c_vp, c_vp]),
     "gsmc_exec_timing": (c_int, [c_vp, c_int]),
     "gsmc_exec_timing_read": (c_int, [c_vp, ctypes.POINTER(ctypes.c_double), c_i64p,
                                       ctypes.POINTER(ctypes.c_double)]),

@@ -222,11 +222,18 @@ class Executor:
 
     __del__ = close
 
-    def run(self, layout, pair_base, out_base, stream_handle):
+    def run(self, layout, pair_base, out_base, stream_handle, flags=None):
         """Enqueue the jobs of ``layout`` whose pairs/outputs live at the given
-        device addresses on ``stream_handle`` (a cudaStream_t as int)."""
+        device addresses on ``stream_handle`` (a cudaStream_t as int).  With
+        ``flags`` (device address of len(jobs) int32) the chunked jobs are
+        checked: flags[k] becomes 1 where job k's chunks did not join its
+        whole-window decode bit for bit."""
         arr = layout.c_jobs(pair_base, out_base)
-        check(_lib.load().gsmc_exec_run(self._h, arr, len(layout.jobs), stream_handle))
+        if flags is None:
+            check(_lib.load().gsmc_exec_run(self._h, arr, len(layout.jobs), stream_handle))
+        else:
+            check(_lib.load().gsmc_exec_run_checked(self._h, arr, len(layout.jobs),
+                                                    stream_handle, flags))
 
     def timing(self, enable):
         check(_lib.load().gsmc_exec_timing(self._h, 1 if enable else 0))
@@ -249,6 +256,13 @@ class DeviceBatch:
     into it on the same stream.  Without ``host`` the outputs stay on the
     device; ``to_host`` then copies them into fresh (pageable) numpy arrays
     through the library's pinned ring.
+
+    Chunked jobs are checked on the device: a job whose chunks' boundary
+    states did not join its whole-window decode bit for bit (rare; the
+    burn-in is ``flank_sites``) is decoded again whole through the context
+    when its results are collected, so every result equals
+    ``FlowContext.run_fb_window`` for the same query exactly.  ``repaired``
+    counts such jobs.
     """
 
     def __init__(self, layout, device):
@@ -257,6 +271,10 @@ class DeviceBatch:
         self.device = torch.device("cuda", device) if isinstance(device, int) else device
         self.h_pairs = torch.empty(max(layout.pair_ints, 1), dtype=torch.int32, pin_memory=True)
         layout.pack_pairs(self.h_pairs.numpy())
+        self.h_flags = torch.zeros(max(len(layout.jobs), 1), dtype=torch.int32, pin_memory=True)
+        self.d_flags = None
+        self.executor = None
+        self.repaired = 0
         self.d_pairs = None
         self.d_out = None
         self.h_out = None
@@ -271,6 +289,8 @@ class DeviceBatch:
                                        device=self.device)
             self.d_out = torch.empty(max(self.layout.out_floats, 1), dtype=torch.float32,
                                      device=self.device)
+            self.d_flags = torch.zeros(max(len(self.layout.jobs), 1), dtype=torch.int32,
+                                       device=self.device)
 
     def launch(self, executor, stream, host=None):
         """Upload pairs, run the jobs, optionally copy the outputs into the
@@ -279,10 +299,12 @@ class DeviceBatch:
         if self.d_out is None:
             self.allocate(stream)
         self.stream = stream
+        self.executor = executor
         with torch.cuda.stream(stream):
             self.d_pairs.copy_(self.h_pairs, non_blocking=True)
             executor.run(self.layout, self.d_pairs.data_ptr(), self.d_out.data_ptr(),
-                         stream.cuda_stream)
+                         stream.cuda_stream, flags=self.d_flags.data_ptr())
+            self.h_flags.copy_(self.d_flags, non_blocking=True)
             if host is not None:
                 self.h_out = host
                 n = self.layout.out_floats
@@ -292,14 +314,35 @@ class DeviceBatch:
             self.done.record(stream)
         return self.done
 
-    def results(self):
-        """Per-job result dicts (views into the pinned host array); waits."""
+    def results(self, redo=None):
+        """Per-job result dicts (views into the pinned host array); waits.
+        Jobs that failed the chunk check are decoded again by ``redo`` (see
+        _redo) and written into their views."""
         if self.h_out is None:
             raise RuntimeError("the batch was launched without a host array; use to_host()")
         self.done.synchronize()
-        return self.layout.results(self.h_out)
+        res = self.layout.results(self.h_out)
+        for k, exact in self._redo(redo):
+            for key, v in res[k].items():
+                v[...] = exact[key]
+        return res
 
-    def to_host(self):
+    def _redo(self, redo=None):
+        """(job index, whole-window result) of the jobs whose chunks failed the
+        device check, decoded again by ``redo(job)`` (default: the context's
+        run_fb_window, so the context must not be busy on another thread);
+        call once the batch is done."""
+        flags = self.h_flags.numpy()[:len(self.layout.jobs)]
+        if redo is None:
+            ctx = self.executor.ctx
+            redo = lambda j: ctx.run_fb_window(j.pairs, j.site_begin, j.site_end,
+                                               mean_only=j.mean_only,
+                                               return_posterior=j.return_posterior)
+        out = [(int(k), redo(self.layout.jobs[int(k)])) for k in np.flatnonzero(flags)]
+        self.repaired = len(out)
+        return out
+
+    def to_host(self, redo=None):
         """Per-job result dicts of new numpy arrays, copied from the device
         outputs once the batch is done (no pinned staging of the results)."""
         res = [{} for _ in self.layout.jobs]
@@ -321,6 +364,9 @@ class DeviceBatch:
         check(_lib.load().gsmc_copy_to_host(
             m, (ctypes.c_void_p * max(m, 1))(*dst), (ctypes.c_void_p * max(m, 1))(*src),
             (ctypes.c_uint64 * max(m, 1))(*nb), self.stream.cuda_stream))
+        self.done.synchronize()
+        for k, exact in self._redo(redo):
+            res[k] = {key: exact[key] for key in res[k]}
         return res
 
 

@@ -56,6 +56,12 @@ struct gsmc_exec {
   int next_image = 0;
   bool use_graph = false;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // reset + scan over image 0 / 1
+  // checked runs (chunking executors): boundary records of the chunked jobs
+  // and, per image, the mapped descriptors the verify kernel reads
+  float2* rec = nullptr;
+  int64_t rec_cap = 0;  // float2
+  ExecCheck* h_check[2] = {nullptr, nullptr};
+  ExecCheck* m_check[2] = {nullptr, nullptr};
   // measurement
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
@@ -104,7 +110,11 @@ void release(gsmc_exec* x) {
     if (x->gexec[i]) cudaGraphExecDestroy(x->gexec[i]);
   cudaFree(x->pool);
   cudaFree(x->d_next);
-  for (int i = 0; i < 2; ++i) cudaFreeHost(x->h_list[i]);
+  cudaFree(x->rec);
+  for (int i = 0; i < 2; ++i) {
+    cudaFreeHost(x->h_list[i]);
+    if (x->h_check[i]) cudaFreeHost(x->h_check[i]);
+  }
   cudaSetDevice(prev);
   delete x;
 }
@@ -154,7 +164,11 @@ int build_graphs(gsmc_exec* x) {
 }
 
 // Tasks of one job: its window cut into chunks, each chunk into pair tiles.
-int job_tasks(const gsmc_exec* x, const gsmc_job& j, int64_t index, std::vector<Task>* out) {
+// With `checks` (a checked run) a chunked job's tasks also write their
+// boundary records into x->rec from float2 *rec_used on, and the job gets a
+// descriptor for the verify kernel.
+int job_tasks(const gsmc_exec* x, const gsmc_job& j, int64_t index, std::vector<Task>* out,
+              int64_t* rec_used = nullptr, std::vector<ExecCheck>* checks = nullptr) {
   const int64_t S = x->v.n_sites;
   if (j.n_pairs < 0) return fail_invalid("job %lld: negative pair count", index);
   if (j.site_begin < 0 || j.site_end > S || j.site_begin > j.site_end)
@@ -174,7 +188,20 @@ int job_tasks(const gsmc_exec* x, const gsmc_job& j, int64_t index, std::vector<
                         index, s1 - s0);
   const int tile = scan_tile_pairs(x->shape);
   const int tf = ((j.flags & GSMC_CI) ? kTaskCI : 0) | ((j.flags & GSMC_POSTERIOR) ? kTaskPosterior : 0);
+  const int64_t n_chunks = (s1 - s0 + core - 1) / core;
+  float2* rec = nullptr;
+  if (checks && n_chunks > 1) {
+    const int64_t need = (n_chunks - 1) * 4 * j.n_pairs;
+    if (*rec_used + need > x->rec_cap)
+      return fail_invalid("job %lld: the run needs more boundary records than the executor "
+                          "holds (%lld float2)", index, x->rec_cap);
+    rec = x->rec + *rec_used;
+    checks->push_back(ExecCheck{*rec_used, (int32_t)(n_chunks - 1), (int32_t)j.n_pairs,
+                                (int32_t)index, 0});
+    *rec_used += need;
+  }
   for (int64_t cs = s0; cs < s1; cs += core) {
+    const int64_t k = (cs - s0) / core;
     const int64_t ce = std::min(s1, cs + core);
     const int64_t ps = std::max(s0, cs - x->flank), pe = std::min(s1, ce + x->flank);
     for (int64_t p = 0; p < j.n_pairs; p += tile) {
@@ -192,13 +219,85 @@ int job_tasks(const gsmc_exec* x, const gsmc_job& j, int64_t index, std::vector<
       t.unscale = 2.0f * x->v.ne;
       t.out_off = j.out_col0 + p;
       t.ldo = j.ld_out;
-      for (int k = 0; k < 5; ++k) {
-        const bool sel = k == 0 || (k < 3 ? (j.flags & GSMC_CI) : (j.flags & GSMC_POSTERIOR));
-        t.out[k] = sel ? j.out[k] : nullptr;
+      for (int o = 0; o < 5; ++o) {
+        const bool sel = o == 0 || (o < 3 ? (j.flags & GSMC_CI) : (j.flags & GSMC_POSTERIOR));
+        t.out[o] = sel ? j.out[o] : nullptr;
+      }
+      if (rec) {
+        t.bl = k > 0 ? rec + (k - 1) * 4 * j.n_pairs + p : nullptr;
+        t.br = k < n_chunks - 1 ? rec + k * 4 * j.n_pairs + p : nullptr;
+        t.bstride = j.n_pairs;
       }
       out->push_back(t);
     }
   }
+  return GSMC_OK;
+}
+
+// One run; with `flags` (device, n_jobs) the chunked jobs are checked.
+int exec_run(gsmc_exec* x, const gsmc_job* jobs, int64_t n_jobs, void* stream, int32_t* flags) {
+  if (!x) return set_error(GSMC_E_INVALID, "null executor");
+  if (n_jobs < 0 || (n_jobs > 0 && !jobs)) return set_error(GSMC_E_INVALID, "bad job list");
+  std::vector<Task> tasks;
+  std::vector<ExecCheck> checks;
+  int64_t rec_used = 0;
+  const bool check = flags && x->rec;
+  for (int64_t i = 0; i < n_jobs; ++i) {
+    const int rc = job_tasks(x, jobs[i], i, &tasks, check ? &rec_used : nullptr,
+                             check ? &checks : nullptr);
+    if (rc) return rc;
+    if ((int64_t)tasks.size() > x->max_tasks)
+      return fail_invalid("the jobs need more than max_tasks = %lld tasks", x->max_tasks);
+  }
+  if (flags && n_jobs > 0) {
+    EXEC_TRY(cudaSetDevice(x->v.device), "cudaSetDevice");
+    EXEC_TRY(cudaMemsetAsync(flags, 0, (size_t)n_jobs * sizeof(int32_t),
+                             static_cast<cudaStream_t>(stream)), "clearing the job flags");
+  }
+  if (tasks.empty()) return GSMC_OK;
+  // longest first: the grid's tail is made of the shortest tasks
+  std::stable_sort(tasks.begin(), tasks.end(), [](const Task& a, const Task& b) {
+    return (a.ce - a.ps) + (a.pe - a.cs) > (b.ce - b.ps) + (b.pe - b.cs);
+  });
+  EXEC_TRY(cudaSetDevice(x->v.device), "cudaSetDevice");
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int img = x->next_image;
+  x->next_image ^= 1;
+  // the last run that read this image must be done before it is rewritten
+  if (x->used[img]) EXEC_TRY(cudaEventSynchronize(x->done[img]), "previous run");
+  unsigned char* h = x->h_list[img];
+  const TaskListHead head{0, (int)tasks.size()};
+  std::memcpy(h, &head, sizeof(head));
+  std::memcpy(h + kTaskListHead, tasks.data(), tasks.size() * sizeof(Task));
+  if (!checks.empty()) std::memcpy(x->h_check[img], checks.data(), checks.size() * sizeof(ExecCheck));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (x->timing) {
+    EXEC_TRY(cudaEventCreate(&e0), "cudaEventCreate");
+    EXEC_TRY(cudaEventCreate(&e1), "cudaEventCreate");
+    EXEC_TRY(cudaEventRecord(e0, st), "cudaEventRecord");
+  }
+  if (x->use_graph) {
+    EXEC_TRY(cudaGraphLaunch(x->gexec[img], st), "cudaGraphLaunch");
+  } else {
+    const int tiles = scan_tiles_per_cta(x->shape);
+    const int grid = (int)std::min<int64_t>(x->grid, ((int64_t)tasks.size() + tiles - 1) / tiles);
+    EXEC_TRY(enqueue_run(x, img, grid, st), "scan launch");
+  }
+  if (!checks.empty()) {
+    int max_pairs = 0;
+    for (const ExecCheck& c : checks) max_pairs = std::max(max_pairs, c.n_pairs);
+    EXEC_TRY(launch_exec_verify(x->rec, x->m_check[img], (int)checks.size(), max_pairs, flags, st),
+             "boundary check");
+    x->launches++;
+  }
+  EXEC_TRY(cudaEventRecord(x->done[img], st), "cudaEventRecord");
+  x->used[img] = true;
+  if (x->timing) {
+    EXEC_TRY(cudaEventRecord(e1, st), "cudaEventRecord");
+    x->events.emplace_back(e0, e1);
+  }
+  x->launches++;
+  for (const Task& t : tasks) x->pair_sites += (double)t.pair_count * (double)(t.ce - t.cs);
   return GSMC_OK;
 }
 
@@ -255,6 +354,22 @@ int gsmc_exec_create(gsmc_ctx* ctx, const gsmc_exec_config* cfg, gsmc_exec** out
     return set_error(GSMC_E_NOMEM, "cudaMalloc of the forward-state pool failed");
   }
   EXEC_TRY(cudaMalloc(&x->d_next, 256), "cudaMalloc of the task counter");
+  if (x->core > 0) {
+    // records of a checked run: (chunks - 1) x 4 per pair of a chunked job,
+    // at most 4 per pair slot of a task
+    x->rec_cap = 4 * x->max_tasks * scan_tile_pairs(x->shape);
+    if (cudaMalloc(&x->rec, (size_t)x->rec_cap * sizeof(float2)) != cudaSuccess) {
+      cudaGetLastError();
+      return set_error(GSMC_E_NOMEM, "cudaMalloc of the boundary records failed");
+    }
+    for (int i = 0; i < 2; ++i) {
+      EXEC_TRY(cudaHostAlloc(&x->h_check[i], (size_t)x->max_tasks * sizeof(ExecCheck),
+                             cudaHostAllocMapped), "cudaHostAlloc");
+      void* dp = nullptr;
+      EXEC_TRY(cudaHostGetDevicePointer(&dp, x->h_check[i], 0), "cudaHostGetDevicePointer");
+      x->m_check[i] = static_cast<ExecCheck*>(dp);
+    }
+  }
   const size_t lb = list_bytes(x->max_tasks);
   for (int i = 0; i < 2; ++i) {
     EXEC_TRY(cudaHostAlloc(&x->h_list[i], lb, cudaHostAllocMapped), "cudaHostAlloc");
@@ -288,52 +403,13 @@ int gsmc_exec_info(const gsmc_exec* x, int* grid, uint64_t* pool_bytes, int64_t*
 }
 
 int gsmc_exec_run(gsmc_exec* x, const gsmc_job* jobs, int64_t n_jobs, void* stream) {
-  if (!x) return set_error(GSMC_E_INVALID, "null executor");
-  if (n_jobs < 0 || (n_jobs > 0 && !jobs)) return set_error(GSMC_E_INVALID, "bad job list");
-  std::vector<Task> tasks;
-  for (int64_t i = 0; i < n_jobs; ++i) {
-    const int rc = job_tasks(x, jobs[i], i, &tasks);
-    if (rc) return rc;
-    if ((int64_t)tasks.size() > x->max_tasks)
-      return fail_invalid("the jobs need more than max_tasks = %lld tasks", x->max_tasks);
-  }
-  if (tasks.empty()) return GSMC_OK;
-  // longest first: the grid's tail is made of the shortest tasks
-  std::stable_sort(tasks.begin(), tasks.end(), [](const Task& a, const Task& b) {
-    return (a.ce - a.ps) + (a.pe - a.cs) > (b.ce - b.ps) + (b.pe - b.cs);
-  });
-  EXEC_TRY(cudaSetDevice(x->v.device), "cudaSetDevice");
-  const cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const int img = x->next_image;
-  x->next_image ^= 1;
-  // the last run that read this image must be done before it is rewritten
-  if (x->used[img]) EXEC_TRY(cudaEventSynchronize(x->done[img]), "previous run");
-  unsigned char* h = x->h_list[img];
-  const TaskListHead head{0, (int)tasks.size()};
-  std::memcpy(h, &head, sizeof(head));
-  std::memcpy(h + kTaskListHead, tasks.data(), tasks.size() * sizeof(Task));
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (x->timing) {
-    EXEC_TRY(cudaEventCreate(&e0), "cudaEventCreate");
-    EXEC_TRY(cudaEventCreate(&e1), "cudaEventCreate");
-    EXEC_TRY(cudaEventRecord(e0, st), "cudaEventRecord");
-  }
-  if (x->use_graph) {
-    EXEC_TRY(cudaGraphLaunch(x->gexec[img], st), "cudaGraphLaunch");
-  } else {
-    const int tiles = scan_tiles_per_cta(x->shape);
-    const int grid = (int)std::min<int64_t>(x->grid, ((int64_t)tasks.size() + tiles - 1) / tiles);
-    EXEC_TRY(enqueue_run(x, img, grid, st), "scan launch");
-  }
-  EXEC_TRY(cudaEventRecord(x->done[img], st), "cudaEventRecord");
-  x->used[img] = true;
-  if (x->timing) {
-    EXEC_TRY(cudaEventRecord(e1, st), "cudaEventRecord");
-    x->events.emplace_back(e0, e1);
-  }
-  x->launches++;
-  for (const Task& t : tasks) x->pair_sites += (double)t.pair_count * (double)(t.ce - t.cs);
-  return GSMC_OK;
+  return exec_run(x, jobs, n_jobs, stream, nullptr);
+}
+
+int gsmc_exec_run_checked(gsmc_exec* x, const gsmc_job* jobs, int64_t n_jobs, void* stream,
+                          int32_t* job_flags) {
+  if (n_jobs > 0 && !job_flags) return set_error(GSMC_E_INVALID, "null job flags");
+  return exec_run(x, jobs, n_jobs, stream, job_flags);
 }
 
 int gsmc_exec_timing(gsmc_exec* x, int enable) {

@@ -119,6 +119,24 @@ __global__ void spec_verify_kernel(const float2* __restrict__ rec, int64_t n_pai
 
 __global__ void add_count_kernel(const int* count, int* acc) { *acc += *count; }
 
+// Thread (pair p, checked job blockIdx.y): any boundary whose exact and
+// speculative states differ flags the job.
+__global__ void exec_verify_kernel(const float2* __restrict__ rec,
+                                   const ExecCheck* __restrict__ checks,
+                                   int32_t* __restrict__ flags) {
+  const ExecCheck& w = checks[blockIdx.y];
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= w.n_pairs) return;
+  const int64_t n = w.n_pairs;
+  for (int b = 0; b < w.n_bnd; ++b) {
+    const float2* r = rec + w.rec_off + (int64_t)b * 4 * n + p;
+    if (!same_bits(r[0], r[n]) || !same_bits(r[2 * n], r[3 * n])) {
+      flags[w.job] = 1;
+      return;
+    }
+  }
+}
+
 // One warp per site row: fold the row's per-warp partials into the site's
 // accumulators.  Lane l sums columns l, l + 32, ... in order, then a fixed
 // shuffle tree combines the lanes, so the result does not depend on timing.
@@ -280,6 +298,14 @@ cudaError_t launch_spec_verify(const float2* rec, int64_t n_pairs, const SpecWin
   if (n_pairs <= 0 || n_win <= 0) return cudaSuccess;
   const dim3 grid((unsigned)((n_pairs + 255) / 256), (unsigned)n_win);
   spec_verify_kernel<<<grid, 256, 0, stream>>>(rec, n_pairs, win, head, repairs, max_repairs);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_exec_verify(const float2* rec, const ExecCheck* checks, int n_checks,
+                               int max_pairs, int32_t* flags, cudaStream_t stream) {
+  if (n_checks <= 0 || max_pairs <= 0) return cudaSuccess;
+  const dim3 grid((unsigned)((max_pairs + 255) / 256), (unsigned)n_checks);
+  exec_verify_kernel<<<grid, 256, 0, stream>>>(rec, checks, flags);
   return cudaGetLastError();
 }
 

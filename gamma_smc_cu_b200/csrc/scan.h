@@ -118,6 +118,23 @@ struct SpecWindow {
   Task repair;
 };
 
+// A job of an executor run whose window was cut into chunks: its boundary
+// records start at float2 `rec_off` of the run's record buffer, laid out
+// [boundary][4 kinds][n_pairs] as the context's speculative chunks.
+struct ExecCheck {
+  int64_t rec_off;
+  int32_t n_bnd;
+  int32_t n_pairs;
+  int32_t job;
+  int32_t pad;
+};
+
+// For every pair of every checked job: compare its boundary records bit for
+// bit and set flags[job] = 1 when any differ (the job's chunked outputs may
+// then differ from its whole-window decode).
+cudaError_t launch_exec_verify(const float2* rec, const ExecCheck* checks, int n_checks,
+                               int max_pairs, int32_t* flags, cudaStream_t stream);
+
 // For every (window, pair) of a speculative launch over n_pairs pairs:
 // compare the boundary records (rec: [boundary][4 kinds][n_pairs] float2) bit
 // for bit and append a one-pair repair task to the list at `head` for each

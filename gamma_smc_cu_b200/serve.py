@@ -188,6 +188,8 @@ class TmrcaServer:
         self._in_use = 0
         self._done = []           # finished requests (for stats)
         self.counters = collections.Counter()
+        self._redo_ex = None
+        self._redo_stream = None
         self._thread = threading.Thread(target=self._loop, name="gsmc-serve", daemon=True)
         self._thread.start()
 
@@ -232,6 +234,8 @@ class TmrcaServer:
             self._thread.join()
         for s in self.slots:
             s.executor.close()
+        if self._redo_ex is not None:
+            self._redo_ex.close()
 
     def __enter__(self):
         return self
@@ -268,10 +272,28 @@ class TmrcaServer:
 
     # ------------------------------------------------------------- scheduler
 
+    def _redo_whole(self, job):
+        """One query decoded as a single whole window (exact), on an executor
+        made on first need: one-warp tiles, no chunking, a pool for at least
+        one CTA of whole-window slots."""
+        if self._redo_ex is None:
+            slot = 4 * max(1, self.ctx.n_sites) * 32 * 8   # 4 one-warp tiles, float2 states
+            self._redo_ex = Executor(self.ctx, tile_width=32, pairs_per_thread=1,
+                                     core_block_sites=0, max_window_sites=self.ctx.n_sites,
+                                     max_tasks=1 << 12, max_pool_bytes=max(1 << 30, slot),
+                                     use_graph=False)
+            self._redo_stream = _new_stream(self.device)
+        b = DeviceBatch(Layout([job]), self.device)
+        b.launch(self._redo_ex, self._redo_stream)
+        return b.to_host()[0]
+
     def _finish(self, slot):
         # views into the batch's pinned host buffer: an arena region returns
         # to the arena once the caller drops the last result array using it
-        results = slot.batch.layout.results(slot.batch.h_out)
+        # done already; queries whose chunks failed the device check are
+        # decoded again whole on the server's own executor (never the context,
+        # which callers may be using on other threads)
+        results = slot.batch.results(redo=self._redo_whole)
         now = time.perf_counter()
         for req, res in zip(slot.requests, results):
             req.t_done = now
@@ -283,6 +305,8 @@ class TmrcaServer:
             self._done.extend((r.t_arrive, r.t_admit, r.t_done, float(r.job.pair_sites))
                               for r in slot.requests)
             self.counters["batches"] += 1
+            if slot.batch.repaired:
+                self.counters["redone_whole"] += slot.batch.repaired
         slot.batch = None
         slot.requests = []
         slot.bytes = 0

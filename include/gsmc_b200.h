@@ -278,6 +278,19 @@ int gsmc_exec_info(const gsmc_exec* exec, int* grid, uint64_t* pool_bytes, int64
  */
 int gsmc_exec_run(gsmc_exec* exec, const gsmc_job* jobs, int64_t n_jobs, void* stream);
 
+/*
+ * gsmc_exec_run that also checks the chunked jobs: job_flags (device memory,
+ * n_jobs int32, cleared by the call on `stream`) gets 1 for every job whose
+ * window was cut into chunks and whose chunks' boundary states (the forward
+ * and backward states each chunk reached from its burn-in against the exact
+ * ones of its neighbours) differ somewhere, bit for bit.  Unflagged jobs'
+ * outputs equal their whole-window decode (gsmc_run_fb_window) exactly; a
+ * flagged job should be decoded again whole (the Python layer does).  No
+ * reference counterpart.
+ */
+int gsmc_exec_run_checked(gsmc_exec* exec, const gsmc_job* jobs, int64_t n_jobs, void* stream,
+                          int32_t* job_flags);
+
 /* Kernel timing of an executor's launches (as gsmc_ctx_timing). */
 int gsmc_exec_timing(gsmc_exec* exec, int enable);
 int gsmc_exec_timing_read(gsmc_exec* exec, double* kernel_ms, int64_t* launches,

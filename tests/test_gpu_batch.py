@@ -3,8 +3,9 @@
 A job (pairs x site window) is decoded as one padded window of the
 reference's block kernels (src/kernels/gamma_smc_flow.cu:632-669, 762-839);
 the oracle's fb_window restates exactly that.  Tolerance: 1e-4 relative on
-every output (the kernels are bit-identical to the oracle, which the exact
-checks assert; chunked jobs are checked against the tolerance only).
+every output, and bit-identical where the kernels are (all of these checks:
+chunked jobs are verified on the device and redone whole when their chunks
+did not join).
 """
 import numpy as np
 import pytest
@@ -122,9 +123,14 @@ def test_executor_reuse_and_two_streams(small_ctx, oracle):
         e.close()
 
 
-def test_chunked_jobs_equal_whole_windows(oracle, flow_field):
-    """Long windows cut into 2,048-site chunks with 2,048 sites of flank agree
-    with the unchunked decode within the tolerance."""
+@pytest.mark.parametrize("flank", [2048, 4])
+def test_chunked_jobs_equal_whole_windows(oracle, flow_field, flank):
+    """Long windows cut into 2,048-site chunks equal the unchunked decode bit
+    for bit: the chunks' boundary states are checked on the device and a job
+    that fails the check (forced here by a 4-site burn-in) is decoded again
+    whole."""
+    import torch
+    from gamma_smc_cu_b200.batch import DeviceBatch, Layout, _count_tasks
     G, pos = synthetic.cohort("chrom", n_sites=12000)
     mu, rho = oracle.estimate_scaled_params(G, pos, 1.25e-8, 1e-8, NE)
     ctx = _core.FlowContext(G, pos, NE, mu, rho, flow_field, 0)
@@ -137,11 +143,22 @@ def test_chunked_jobs_equal_whole_windows(oracle, flow_field):
         s0 = int(rng.integers(0, 12000 - w + 1))
         jobs.append(Job(allp[rng.choice(len(allp), n, replace=False)], s0, s0 + w,
                         mean_only=k % 2 == 0, return_posterior=k % 4 == 1))
-    chunked = run_jobs(ctx, jobs, core_block_sites=2048, flank_sites=2048)
+    cfg = dict(core_block_sites=2048, flank_sites=flank)
+    ex = Executor(ctx, max_tasks=_count_tasks(jobs, cfg) + 8, **cfg)
+    b = DeviceBatch(Layout(jobs), ctx.device_id)
+    b.launch(ex, torch.cuda.current_stream(torch.device("cuda", ctx.device_id)))
+    chunked = b.to_host()
+    if flank == 4:
+        assert b.repaired > 0
     for j, r in zip(jobs, chunked):
         want = ctx.run_fb_window(j.pairs, j.site_begin, j.site_end, mean_only=j.mean_only,
                                  return_posterior=j.return_posterior)
-        _check(r, want, exact=False)
+        _check(r, want, exact=True)
+    ex.close()
+    if flank == 2048:
+        for j, r in zip(jobs, run_jobs(ctx, jobs, **cfg)):
+            _check(r, ctx.run_fb_window(j.pairs, j.site_begin, j.site_end, mean_only=j.mean_only,
+                                        return_posterior=j.return_posterior), exact=True)
 
 
 def test_job_errors(small_ctx):

@@ -77,14 +77,21 @@ def test_served_results_equal_alone(small_data, oracle, flow_field):
     assert st["batches"] <= st["completed"]
 
 
-def test_served_chunked_windows_within_tolerance(oracle, flow_field):
+@pytest.mark.parametrize("flank", [2048, 4])
+def test_served_chunked_windows_exact(oracle, flow_field, flank):
+    """Chunked windows in the served mix equal the query decoded alone bit for
+    bit; a 4-site burn-in makes chunks fail the device check and the server
+    redo those queries whole."""
     G, pos = synthetic.cohort("chrom", n_sites=12000)
     mu, rho = oracle.estimate_scaled_params(G, pos, 1.25e-8, 1e-8, NE)
     ctx = _core.FlowContext(G, pos, NE, mu, rho, flow_field, 0)
     with TmrcaServer(ctx, positions=pos, max_inflight=2, core_block_sites=2048,
-                     tile_width=32) as srv:
+                     flank_sites=flank, tile_width=32) as srv:
         subs = _mix(srv, G.shape[0], G.shape[1], clients=2, per_client=10, max_pairs=200)
-        _check_alone(ctx, subs, exact=False)
+        _check_alone(ctx, subs, exact=True)
+        st = srv.stats()
+    if flank == 4:
+        assert st.get("redone_whole", 0) > 0
 
 
 def test_server_rejects_query_beyond_budget(small_data, oracle, flow_field):

@@ -112,3 +112,20 @@ def test_job_mix_bp_windows_cover_their_sequence():
     widths = [j["site_end"] - j["site_begin"] for j in jobs]
     assert max(widths) < S and min(widths) >= 1   # 200 kb of a 1 Mb sequence at most
     assert synthetic.job_mix_bp(pos, G.shape[0], 512, seed=5)[7]["site_begin"] == jobs[7]["site_begin"]
+
+
+def test_layout_floats_match_job_padding():
+    """The server admits queries by Job.layout_floats; a batch's buffer is the
+    sum of those (every output region padded to the layout's alignment)."""
+    from gamma_smc_cu_b200.batch import Job, Layout
+    rng = np.random.default_rng(3)
+    jobs = []
+    for k in range(40):
+        n = int(rng.integers(1, 70))
+        s0 = int(rng.integers(0, 400))
+        jobs.append(Job(np.stack([rng.integers(1, 20, n), np.zeros(n, int)], 1), s0,
+                        s0 + int(rng.integers(1, 300)), mean_only=k % 3 != 0,
+                        return_posterior=k % 4 == 1))
+    lay = Layout(jobs)
+    assert lay.out_floats == sum(j.layout_floats for j in jobs)
+    assert all(j.layout_floats >= j.output_floats for j in jobs)

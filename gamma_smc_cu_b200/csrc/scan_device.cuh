@@ -213,11 +213,13 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   float2* fp = slot + j0;
   // Gap codes run two sites ahead: `cur` is this site's, `nx` the next one's
   // (already in registers, so the next-site prefetch does not wait on it).
-  auto fwd_step = [&](int s, SiteCode sc, int next_layer) {
-    if ((s & 63) == 0 && s != ps) {
+  // het words: the loops below run in 64-site word blocks and reload at each
+  // block's first site (the first site of the task comes preloaded)
+  auto reload = [&](int s) {
 #pragma unroll
-      for (int k = 0; k < NP; ++k) x[k] = word_at(gi[k], nh, s) ^ word_at(gj[k], nh, s);
-    }
+    for (int k = 0; k < NP; ++k) x[k] = word_at(gi[k], nh, s) ^ word_at(gj[k], nh, s);
+  };
+  auto fwd_step = [&](int s, SiteCode sc, int next_layer) {
     if (sc.chunks) {
       for (int u = 0; u < sc.chunks; ++u) {
 #pragma unroll
@@ -251,11 +253,14 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     for (int k = 0; k < NP; ++k) __stcs(fp + k * WIDTH, make_float2(m[k], c[k]));
     fp += kRow;
   }
-  for (++s; s < cs; ++s) {
-    const SiteCode nx2 = code[s + 2];
-    fwd_step(s, cur, nx.layer);
-    cur = nx;
-    nx = nx2;
+  for (++s; s < cs;) {
+    if ((s & 63) == 0) reload(s);
+    for (const int e = min(cs, (s | 63) + 1); s < e; ++s) {
+      const SiteCode nx2 = code[s + 2];
+      fwd_step(s, cur, nx.layer);
+      cur = nx;
+      nx = nx2;
+    }
   }
   // boundary records of a speculative chunk (see Task); lanes past the task's
   // last pair write nothing
@@ -267,14 +272,17 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     }
   };
   if (t.bl) record(t.bl, 1);
-  for (; s < ce; ++s) {
-    const SiteCode nx2 = code[s + 2];
-    fwd_step(s, cur, nx.layer);
-    cur = nx;
-    nx = nx2;
+  while (s < ce) {
+    if ((s & 63) == 0 && s != ps) reload(s);
+    for (const int e = min(ce, (s | 63) + 1); s < e; ++s) {
+      const SiteCode nx2 = code[s + 2];
+      fwd_step(s, cur, nx.layer);
+      cur = nx;
+      nx = nx2;
 #pragma unroll
-    for (int k = 0; k < NP; ++k) __stcs(fp + k * WIDTH, make_float2(m[k], c[k]));
-    fp += kRow;
+      for (int k = 0; k < NP; ++k) __stcs(fp + k * WIDTH, make_float2(m[k], c[k]));
+      fp += kRow;
+    }
   }
   if (t.br) record(t.br, 0);
 
@@ -288,10 +296,6 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   // Backward step at site s: the het/hom site table first, then any full
   // 1000-bp chunks.
   auto bwd_fetch = [&](int s, SiteCode sc, int next_layer, Fetch* f) {
-    if ((s & 63) == 63 && s != pe - 1) {
-#pragma unroll
-      for (int k = 0; k < NP; ++k) x[k] = word_at(gi[k], nh, s) ^ word_at(gj[k], nh, s);
-    }
     const float4* layer = bwd_tab + sc.layer;
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
@@ -314,13 +318,16 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   s = pe - 1;
   cur = code[s];
   nx = code[s - 1];
-  for (; s >= ce; --s) {
-    const SiteCode nx2 = code[s - 2];
-    Fetch f[NP];
-    bwd_fetch(s, cur, nx.layer, f);
-    bwd_finish(cur, f);
-    cur = nx;
-    nx = nx2;
+  while (s >= ce) {
+    if ((s & 63) == 63 && s != pe - 1) reload(s);
+    for (const int e = max(ce, s & ~63); s >= e; --s) {
+      const SiteCode nx2 = code[s - 2];
+      Fetch f[NP];
+      bwd_fetch(s, cur, nx.layer, f);
+      bwd_finish(cur, f);
+      cur = nx;
+      nx = nx2;
+    }
   }
   if (t.br) record(t.br, 3);
   // forward-state ring: q[i] holds the state of site s - i
@@ -334,9 +341,12 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     fq -= kRow;
   }
   int64_t o = t.out_off + (int64_t)(ce - 1 - t.out_row0) * t.ldo + j0;
+  s = ce - 1;
+  while (s >= cs) {
+  if ((s & 63) == 63 && s != pe - 1) reload(s);
   // unrolled by the ring depth so the ring rotation is register renaming
 #pragma unroll kFwdPrefetch
-  for (s = ce - 1; s >= cs; --s) {
+  for (const int e = max(cs, s & ~63); s >= e; --s) {
     float2 f[NP];
 #pragma unroll
     for (int k = 0; k < NP; ++k) f[k] = q[0][k];
@@ -400,6 +410,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     }
     cur = nx;
     nx = nx2;
+  }
   }
   if (t.bl) {
     // the backward state after applying site cs itself, for the left neighbour

@@ -203,21 +203,23 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
 
   // ---- forward: [ps, ce); states stored for [cs, ce) ----
   float m[NP], c[NP];
-  uint64_t x[NP];
+  uint32_t x[NP];
 #pragma unroll
   for (int k = 0; k < NP; ++k) {
     m[k] = 0.0f;
     c[k] = 0.0f;
-    x[k] = (word_at(gi[k], nh, ps) ^ word_at(gj[k], nh, ps)) >> (ps & 63);
+    x[k] = (uint32_t)((word_at(gi[k], nh, ps) ^ word_at(gj[k], nh, ps)) >> (ps & 63));
   }
   float2* fp = slot + j0;
   // Gap codes run two sites ahead: `cur` is this site's, `nx` the next one's
   // (already in registers, so the next-site prefetch does not wait on it).
-  // het words: the loops below run in 64-site word blocks and reload at each
+  // het bits: 32-bit halves of the pair's XORed genotype words (a 32-bit
+  // shift per site); the loops below run in 32-site blocks and reload at each
   // block's first site (the first site of the task comes preloaded)
   auto reload = [&](int s) {
 #pragma unroll
-    for (int k = 0; k < NP; ++k) x[k] = word_at(gi[k], nh, s) ^ word_at(gj[k], nh, s);
+    for (int k = 0; k < NP; ++k)
+      x[k] = (uint32_t)((word_at(gi[k], nh, s) ^ word_at(gj[k], nh, s)) >> (s & 32));
   };
   auto fwd_step = [&](int s, SiteCode sc, int next_layer) {
     if (sc.chunks) {
@@ -230,10 +232,10 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     Fetch f[NP];
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
-      const int het = (int)(x[k] & 1ull);
+      const int het = (int)(x[k] & 1u);
       x[k] >>= 1;
       f[k] = patch_fetch(layer + het * kHetF4, m[k], c[k]);
-      prefetch_patch(fwd_tab + next_layer + (int)(x[k] & 1ull) * kHetF4 + kPatchF4 * f[k].idx);
+      prefetch_patch(fwd_tab + next_layer + (int)(x[k] & 1u) * kHetF4 + kPatchF4 * f[k].idx);
     }
 #pragma unroll
     for (int k = 0; k < NP; ++k) patch_interp(f[k], m[k], c[k]);
@@ -254,8 +256,8 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     fp += kRow;
   }
   for (++s; s < cs;) {
-    if ((s & 63) == 0) reload(s);
-    for (const int e = min(cs, (s | 63) + 1); s < e; ++s) {
+    if ((s & 31) == 0) reload(s);
+    for (const int e = min(cs, (s | 31) + 1); s < e; ++s) {
       const SiteCode nx2 = code[s + 2];
       fwd_step(s, cur, nx.layer);
       cur = nx;
@@ -273,8 +275,8 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   };
   if (t.bl) record(t.bl, 1);
   while (s < ce) {
-    if ((s & 63) == 0 && s != ps) reload(s);
-    for (const int e = min(ce, (s | 63) + 1); s < e; ++s) {
+    if ((s & 31) == 0 && s != ps) reload(s);
+    for (const int e = min(ce, (s | 31) + 1); s < e; ++s) {
       const SiteCode nx2 = code[s + 2];
       fwd_step(s, cur, nx.layer);
       cur = nx;
@@ -291,7 +293,8 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   for (int k = 0; k < NP; ++k) {
     m[k] = 0.0f;
     c[k] = 0.0f;
-    x[k] = (word_at(gi[k], nh, pe - 1) ^ word_at(gj[k], nh, pe - 1)) << (63 - ((pe - 1) & 63));
+    x[k] = (uint32_t)((word_at(gi[k], nh, pe - 1) ^ word_at(gj[k], nh, pe - 1)) >> ((pe - 1) & 32))
+           << (31 - ((pe - 1) & 31));
   }
   // Backward step at site s: the het/hom site table first, then any full
   // 1000-bp chunks.
@@ -299,10 +302,10 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     const float4* layer = bwd_tab + sc.layer;
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
-      const int het = (int)(x[k] >> 63);
+      const int het = (int)(x[k] >> 31);
       x[k] <<= 1;
       f[k] = patch_fetch(layer + het * kHetF4, m[k], c[k]);
-      prefetch_patch(bwd_tab + next_layer + (int)(x[k] >> 63) * kHetF4 + kPatchF4 * f[k].idx);
+      prefetch_patch(bwd_tab + next_layer + (int)(x[k] >> 31) * kHetF4 + kPatchF4 * f[k].idx);
     }
   };
   auto bwd_finish = [&](SiteCode sc, const Fetch* f) {
@@ -319,8 +322,8 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   cur = code[s];
   nx = code[s - 1];
   while (s >= ce) {
-    if ((s & 63) == 63 && s != pe - 1) reload(s);
-    for (const int e = max(ce, s & ~63); s >= e; --s) {
+    if ((s & 31) == 31 && s != pe - 1) reload(s);
+    for (const int e = max(ce, s & ~31); s >= e; --s) {
       const SiteCode nx2 = code[s - 2];
       Fetch f[NP];
       bwd_fetch(s, cur, nx.layer, f);
@@ -343,10 +346,10 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   int64_t o = t.out_off + (int64_t)(ce - 1 - t.out_row0) * t.ldo + j0;
   s = ce - 1;
   while (s >= cs) {
-  if ((s & 63) == 63 && s != pe - 1) reload(s);
+  if ((s & 31) == 31 && s != pe - 1) reload(s);
   // unrolled by the ring depth so the ring rotation is register renaming
 #pragma unroll kFwdPrefetch
-  for (const int e = max(cs, s & ~63); s >= e; --s) {
+  for (const int e = max(cs, s & ~31); s >= e; --s) {
     float2 f[NP];
 #pragma unroll
     for (int k = 0; k < NP; ++k) f[k] = q[0][k];

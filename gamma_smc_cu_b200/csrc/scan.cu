@@ -31,8 +31,9 @@ namespace {
 // left; its forward-state slot is reused task after task.
 // Resident CTAs per SM the register budget is fitted to (128 threads each).
 // The scan is bound by the latency of its lookup chain and by issue, so warps
-// per SM matter.  One pair per thread: 10 CTAs (48 registers with a one-deep
-// forward-state ring, no spill; 9 CTAs at 56 registers ran level, 7-8 slower).
+// per SM matter.  One pair per thread: 10 CTAs (46-48 registers with a
+// one-deep forward-state ring, no spill; 9 CTAs at 56 registers ran level,
+// 7-8 slower).
 // Two pairs per thread: 8 CTAs (64 registers, no spill) measured 3% faster
 // than 7 (69-72 registers).
 #ifndef GSMC_MIN_CTAS

@@ -278,10 +278,11 @@ class TmrcaServer:
         one CTA of whole-window slots."""
         if self._redo_ex is None:
             slot = 4 * max(1, self.ctx.n_sites) * 32 * 8   # 4 one-warp tiles, float2 states
+            n_pairs = self.ctx.n_haps * (self.ctx.n_haps - 1) // 2
             self._redo_ex = Executor(self.ctx, tile_width=32, pairs_per_thread=1,
                                      core_block_sites=0, max_window_sites=self.ctx.n_sites,
-                                     max_tasks=1 << 12, max_pool_bytes=max(1 << 30, slot),
-                                     use_graph=False)
+                                     max_tasks=max(1 << 12, -(-n_pairs // 32)),
+                                     max_pool_bytes=max(1 << 30, slot), use_graph=False)
             self._redo_stream = _new_stream(self.device)
         b = DeviceBatch(Layout([job]), self.device)
         b.launch(self._redo_ex, self._redo_stream)
@@ -293,9 +294,16 @@ class TmrcaServer:
         # done already; queries whose chunks failed the device check are
         # decoded again whole on the server's own executor (never the context,
         # which callers may be using on other threads)
-        results = slot.batch.results(redo=self._redo_whole)
+        try:
+            results = slot.batch.results(redo=self._redo_whole)
+        except Exception as e:  # a failed redo fails only its batch
+            results = None
+            for req in slot.requests:
+                req.future.set_exception(e)
+            with self._cv:
+                self.counters["failed"] += len(slot.requests)
         now = time.perf_counter()
-        for req, res in zip(slot.requests, results):
+        for req, res in zip(slot.requests, results or []):
             req.t_done = now
             req.future.set_result(res)
         with self._cv:
@@ -303,7 +311,7 @@ class TmrcaServer:
             # timings only: the requests (and the results their futures hold)
             # are not kept, so result memory returns once the caller drops it
             self._done.extend((r.t_arrive, r.t_admit, r.t_done, float(r.job.pair_sites))
-                              for r in slot.requests)
+                              for r in slot.requests if r.t_done is not None)
             self.counters["batches"] += 1
             if slot.batch.repaired:
                 self.counters["redone_whole"] += slot.batch.repaired

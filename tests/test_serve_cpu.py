@@ -63,6 +63,7 @@ class Recorder:
     launches = 0
     max_bytes = 0
     fail_tag = None
+    fail_results_tag = None
     delay = 0.01
     lock = threading.Lock()
 
@@ -76,6 +77,10 @@ def make_batch_cls(rec, server_ref):
             self.done = None
 
         def results(self, redo=None):
+            for j in self.layout.jobs:
+                if (rec.fail_results_tag is not None and j.pairs.size
+                        and j.pairs[0, 0] == rec.fail_results_tag):
+                    raise RuntimeError("injected collection failure")
             return self.layout.results(self.h_out)
 
         def launch(self, executor, stream, host=None):
@@ -266,3 +271,17 @@ def test_batches_fit_the_arena_when_results_are_dropped(server_factory):
     st = s.stats()
     assert st.get("outside_arena", 0) == 0
     assert rec.launches >= n * 3200 // 16384
+
+
+def test_collection_failure_fails_only_its_batch(server_factory):
+    """A batch whose results cannot be collected (e.g. a failed whole-window
+    redo) fails its own queries; the server keeps serving."""
+    s, rec = server_factory(max_inflight=1)
+    rec.fail_results_tag = 17
+    bad = s.submit([(17, 0)], 0, 50)
+    with pytest.raises(RuntimeError, match="injected collection"):
+        bad.result(timeout=10)
+    rec.fail_results_tag = None
+    _check_result(s.submit([(3, 1)], 10, 60), 3, 10, 60, 1, ("mean",))
+    st = s.stats()
+    assert st["failed"] >= 1 and st["completed"] >= 1

@@ -47,9 +47,9 @@ UNIT = "pair-sites/s"
 BYTES_MEAN_ONLY = 4.25      # 4 B fp32 mean + 2 genotype bits per pair-site
 BYTES_FULL_POSTERIOR = 12.25
 # DRAM bytes (read + write) the scan kernel moves per core pair-site in
-# mean-only mode, from an ncu capture of the same kernel on 6,144 sites x
-# 63,190 pairs (profiles/fb_scan_persistent_scan_case.md): 16 B forward-state
-# round trip + 4 B output.
+# mean-only mode, from an ncu capture of the same kernel on the first 8,192
+# sites x 63,190 pairs (`--case scan`): 16 B forward-state round trip + 4 B
+# output.
 TRAFFIC_PER_PAIR_SITE = 20.0
 
 
@@ -71,6 +71,9 @@ def parse():
                     help="skip the 2,000-haplotype x 1,000,000-pair streamed run")
     ap.add_argument("--plain-jobs", type=int, default=48,
                     help="jobs of the mix timed through the plain per-call path")
+    ap.add_argument("--case", default=None,
+                    help="run one small profiling case instead of the benchmark")
+    ap.add_argument("--repeat", type=int, default=1, help="repetitions of --case")
     return ap.parse_args()
 
 
@@ -228,6 +231,10 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.case:
+        CASES[args.case](args.repeat)
+        print(f"{args.case}: ok")
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
@@ -742,6 +749,149 @@ def run_e2e(G, pos, pairs, core, flank, steps):
     return {"value": P * sites / t, "unit": UNIT, "h2d_bytes_per_step": int(Gs.nbytes + ps.nbytes + 8 * P),
             "d2h_bytes_per_step": int(4 * sites * P), "seconds_per_step": t, "sites": sites,
             "steps": len(times)}
+
+
+# ------------------------------------------------------------ profiling cases
+# Small, self-contained runs of each kernel for profilers (`--case NAME
+# [--repeat N]`): each builds its inputs, runs once to warm up and then
+# `--repeat` more times.  Inputs/outputs stay above the 126 MB L2 (so DRAM
+# counters mean something) while the device holds a few GB at most.
+#   scan      cached FB, chromosome cohort, 8,192 sites x 63,190 pairs,
+#             blockwise core 512 / flank 128 (16 windows x 247 tiles of 256
+#             pairs: the two-pairs-per-thread shape of the full job), mean-only
+#   full      cached FB, mean + alpha + beta, 4,096 sites x 63,190 pairs,
+#             blockwise core 256 / flank 64 (16 windows, two pairs per thread)
+#   batch     64 uneven jobs (1-2,000 pairs, 2k-40k-site windows) over a
+#             60,000-site slice, one executor launch (32-thread tiles,
+#             4,096-site chunks)
+#   summary   per-site summary, 16,384 pairs x 20,000 sites (8,192 / 2,048)
+#   fwd       forward-only posterior, 8,192 pairs x 20,000 sites
+#   uncached  uncached flow-field FB, 4,096 pairs x 10,000 sites
+#   flowgen   GPU flow-field generation, 51 x 50 cells, constant Ne
+#   fwd_spec  forward-only posterior, 2,000 pairs x 400,000 sites (exact
+#             speculative site chunks)
+#   uncached_spec  uncached flow-field FB, 500 pairs x 200,000 sites (same)
+
+def _case_ctx(n_sites):
+    from gamma_smc_cu_b200 import _core, synthetic
+    from gamma_smc_cu_b200.infer import _estimate_scaled_params
+    G, pos = synthetic.cohort("chrom", n_sites=n_sites)
+    mu, rho = _estimate_scaled_params(G, pos, 1.25e-8, 1e-8, 1e4)
+    return _core.FlowContext(G, pos, 1e4, mu, rho, _core.DEFAULT_FLOW_FIELD, 0), G, pos
+
+
+def case_scan(repeat):
+    import torch
+    from gamma_smc_cu_b200 import _lib, synthetic
+    ctx, G, pos = _case_ctx(8192)
+    pairs = synthetic.all_pairs(G.shape[0])
+    dev = torch.device("cuda", ctx.device_id)
+    pi = torch.from_numpy(np.ascontiguousarray(pairs[:, 0])).to(dev)
+    pj = torch.from_numpy(np.ascontiguousarray(pairs[:, 1])).to(dev)
+    out = torch.empty((G.shape[1], len(pairs)), device=dev)
+    L = _lib.load()
+    for _ in range(1 + repeat):
+        _lib.check(L.gsmc_run_fb_blockwise_device(
+            ctx.handle, pi.data_ptr(), pj.data_ptr(), len(pairs), 512, 128, 0,
+            out.data_ptr(), None, None, None, None, len(pairs), 0, None))
+    torch.cuda.synchronize()
+    print("scan shape", ctx.scan_shape())
+
+
+def case_full(repeat):
+    import torch
+    from gamma_smc_cu_b200 import _lib, synthetic
+    ctx, G, pos = _case_ctx(4096)
+    pairs = synthetic.all_pairs(G.shape[0])
+    dev = torch.device("cuda", ctx.device_id)
+    pi = torch.from_numpy(np.ascontiguousarray(pairs[:, 0])).to(dev)
+    pj = torch.from_numpy(np.ascontiguousarray(pairs[:, 1])).to(dev)
+    outs = [torch.empty((G.shape[1], len(pairs)), device=dev) for _ in range(3)]
+    L = _lib.load()
+    for _ in range(1 + repeat):
+        _lib.check(L.gsmc_run_fb_blockwise_device(
+            ctx.handle, pi.data_ptr(), pj.data_ptr(), len(pairs), 256, 64, _lib.GSMC_POSTERIOR,
+            outs[0].data_ptr(), None, None, outs[1].data_ptr(), outs[2].data_ptr(), len(pairs), 0,
+            None))
+    torch.cuda.synchronize()
+    print("scan shape", ctx.scan_shape())
+
+
+def case_batch(repeat):
+    import torch
+    from gamma_smc_cu_b200.batch import DeviceBatch, Executor, Job, Layout, _count_tasks
+    from gamma_smc_cu_b200 import synthetic
+    ctx, G, pos = _case_ctx(60000)
+    jobs = [Job(**j) for j in synthetic.job_mix(G.shape[0], G.shape[1], 64, seed=5,
+                                                 pairs_range=(1, 2000),
+                                                 window_range=(2000, 40000))]
+    cfg = dict(tile_width=32, pairs_per_thread=1, core_block_sites=4096, flank_sites=2048)
+    ex = Executor(ctx, max_tasks=_count_tasks(jobs, cfg) + 16, **cfg)
+    st = torch.cuda.Stream(torch.device("cuda", ctx.device_id))
+    b = DeviceBatch(Layout(jobs), ctx.device_id)
+    b.allocate(st)
+    with torch.cuda.stream(st):
+        b.d_pairs.copy_(b.h_pairs, non_blocking=True)
+    for _ in range(1 + repeat):
+        ex.run(b.layout, b.d_pairs.data_ptr(), b.d_out.data_ptr(), st.cuda_stream)
+    st.synchronize()
+    ex.close()
+
+
+def case_summary(repeat):
+    from gamma_smc_cu_b200 import synthetic
+    ctx, G, pos = _case_ctx(20000)
+    pairs = synthetic.random_pairs(G.shape[0], 16384, 3)
+    for _ in range(1 + repeat):
+        ctx.run_fb_summary(pairs, core_block_sites=8192, flank_sites=2048)
+
+
+def case_fwd(repeat):
+    from gamma_smc_cu_b200 import synthetic
+    ctx, G, pos = _case_ctx(20000)
+    pairs = synthetic.random_pairs(G.shape[0], 8192, 4)
+    for _ in range(1 + repeat):
+        ctx.run_fwd(pairs)
+
+
+def case_uncached(repeat):
+    from gamma_smc_cu_b200 import _core, synthetic
+    G, pos = synthetic.cohort("chrom", n_sites=10000)
+    pairs = synthetic.random_pairs(G.shape[0], 4096, 6)
+    for _ in range(1 + repeat):
+        _core.gamma_smc_flow_fb(G, pos, pairs, mean_only=True)
+
+
+def case_flowgen(repeat):
+    from gamma_smc_cu_b200.demographic import generate_flow_field
+    for _ in range(1 + repeat):
+        generate_flow_field(verbose=False)
+
+
+def case_fwd_spec(repeat):
+    from gamma_smc_cu_b200 import synthetic
+    ctx, G, pos = _case_ctx(400000)
+    pairs = synthetic.random_pairs(G.shape[0], 2000, 4)
+    for _ in range(1 + repeat):
+        ctx.run_fwd(pairs)
+
+
+def case_uncached_spec(repeat):
+    from gamma_smc_cu_b200 import _core, synthetic
+    G, pos = synthetic.cohort("chrom", n_sites=200000)
+    pairs = synthetic.random_pairs(G.shape[0], 500, 4)
+    for _ in range(1 + repeat):
+        _core.gamma_smc_flow_fb(G, pos, pairs, mean_only=True)
+
+
+CASES = {"scan": case_scan, "full": case_full, "batch": case_batch, "summary": case_summary, "fwd": case_fwd,
+         "uncached": case_uncached, "flowgen": case_flowgen, "fwd_spec": case_fwd_spec,
+         "uncached_spec": case_uncached_spec}
+
+
+CASES = {"scan": case_scan, "full": case_full, "batch": case_batch, "summary": case_summary,
+         "fwd": case_fwd, "uncached": case_uncached, "flowgen": case_flowgen,
+         "fwd_spec": case_fwd_spec, "uncached_spec": case_uncached_spec}
 
 
 if __name__ == "__main__":

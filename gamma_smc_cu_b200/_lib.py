@@ -125,6 +125,7 @@ SIGNATURES = {
     "gsmc_ctx_timing": (c_int, [c_vp, c_int]),
     "gsmc_ctx_timing_read": (c_int, [c_vp, ctypes.POINTER(ctypes.c_double), c_i64p,
                                      ctypes.POINTER(ctypes.c_double)]),
+    "gsmc_set_copy_wait_polls": (c_int, [c_i64, c_i64p]),
     "gsmc_bitpack": (c_int, [c_u8p, c_i64, c_i64, c_u64p]),
     "gsmc_unpack": (c_int, [c_u64p, c_i64, c_i64, c_u8p]),
     "gsmc_ctx_table_layer": (c_int, [c_vp, c_int, c_int, c_f32p]),

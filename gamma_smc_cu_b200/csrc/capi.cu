@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -23,6 +24,7 @@
 #include "scan.h"
 #include "tables.h"
 #include "uncached.h"
+#include "windows.h"
 
 using namespace gsmc;
 
@@ -36,6 +38,9 @@ struct FlowFbStats {
   int64_t repaired = 0;
 };
 thread_local FlowFbStats g_flow_fb_stats;
+
+// mbarrier polls the uncached kernels wait for their flow-field copy.
+std::atomic<long long> g_copy_wait_polls{kDefaultCopyWaitPolls};
 
 int fail(int code, const char* fmt, ...) {
   char buf[1024];
@@ -151,9 +156,11 @@ struct Block {
 // Windows core +/- flank clamped to [0, S) (src/bindings.cpp:2517-2534).
 std::vector<Block> make_windows(int64_t S, int64_t core, int64_t flank) {
   std::vector<Block> out;
-  for (int64_t cs = 0; cs < S; cs += core) {
-    const int64_t ce = std::min(S, cs + core);
-    out.push_back({cs, ce, std::max<int64_t>(0, cs - flank), std::min(S, ce + flank)});
+  const int64_t n = window_count(S, core);
+  out.reserve((size_t)n);
+  for (int64_t w = 0; w < n; ++w) {
+    const WindowBounds b = window_bounds(w, S, core, flank);
+    out.push_back({b.cs, b.ce, b.ps, b.pe});
   }
   return out;
 }
@@ -1661,6 +1668,7 @@ int gsmc_flow_fb(const uint8_t* G, int64_t n_haps, int64_t n_sites, const double
     a.upper = ci ? b.out + (size_t)2 * n_sites * n : nullptr;
     a.ldo = n;
     a.error = b.error;
+    a.wait_polls = g_copy_wait_polls.load();
     UncachedSpec sp;
     std::memset(&sp, 0, sizeof(sp));
     sp.k_chunks = std::min(k_max, chunks_for(n));
@@ -1693,6 +1701,13 @@ int gsmc_flow_fb(const uint8_t* G, int64_t n_haps, int64_t n_sites, const double
     CUDA_TRY(cudaMemcpy(&repaired, b.rep, sizeof(int), cudaMemcpyDeviceToHost));
     g_flow_fb_stats.repaired = repaired;
   }
+  return GSMC_OK;
+}
+
+int gsmc_set_copy_wait_polls(int64_t polls, int64_t* previous) {
+  if (polls < 0) return fail(GSMC_E_INVALID, "the poll budget must be non-negative");
+  const long long prev = g_copy_wait_polls.exchange(polls);
+  if (previous) *previous = prev;
   return GSMC_OK;
 }
 

@@ -23,8 +23,10 @@
 //   caller; the counter is cleared at the start of every call and the slots
 //   need no clearing (each task writes its slot rows before reading them);
 // * the first call on a device looks the array's address up with
-//   cudaGetSymbolAddress (loading this file's device code if needed); make
-//   that first call before capturing any stream.
+//   cudaGetSymbolAddress (loading this file's device code if needed) and
+//   keeps it for the life of the process; make that first call before
+//   capturing any stream, and do not call this entry point on a device after
+//   a cudaDeviceReset, which would leave the kept address stale.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,6 +39,7 @@
 #include "scan.h"
 #include "scan_device.cuh"
 #include "tables.h"
+#include "windows.h"
 
 namespace gsmc {
 namespace {
@@ -56,9 +59,9 @@ struct NoAllocArgs {
   int* counter;    // in the scratch, cleared before the launch
   float2* slots;   // in the scratch
   int64_t slot_rows;
-  int n_sites;
-  int core;
-  int flank;
+  int64_t n_sites;
+  int64_t core;    // clamped to [1, n_sites] on the host
+  int64_t flank;   // clamped to [0, n_sites] on the host
   int n_pairs;
   int tiles;       // pair tiles per window
   int n_tasks;     // windows x tiles
@@ -81,12 +84,12 @@ __global__ void __launch_bounds__(kThreads) fb_scan_noalloc(const NoAllocArgs a)
       id = atomicAdd(a.counter, 1);
       if (id < a.n_tasks) {
         const int w = id / a.tiles, tile = id % a.tiles;
-        const int cs = w * a.core;
-        const int ce = min(a.n_sites, cs + a.core);
-        task.ps = max(0, cs - a.flank);
-        task.cs = cs;
-        task.ce = ce;
-        task.pe = min(a.n_sites, ce + a.flank);
+        // int64 window arithmetic: every bound lies in [0, n_sites] < 2^31
+        const WindowBounds b = window_bounds(w, a.n_sites, a.core, a.flank);
+        task.ps = (int32_t)b.ps;
+        task.cs = (int32_t)b.cs;
+        task.ce = (int32_t)b.ce;
+        task.pe = (int32_t)b.pe;
         task.pi = a.pi + (int64_t)tile * kThreads;
         task.pj = a.pj + (int64_t)tile * kThreads;
         task.pair_count = min(kThreads, a.n_pairs - tile * kThreads);
@@ -155,7 +158,10 @@ extern "C" int gsmc_run_fb_blockwise_device_noalloc(
   const int64_t S = v.n_sites;
   if (S >= 0x7fffffff) return set_error(GSMC_E_INVALID, "too many sites for one call");
   if (n_pairs == 0 || S == 0) return GSMC_OK;
-  const int64_t core = std::min<int64_t>(core_block_sites, S);
+  // Core and flank clamped to the sequence in int64 before anything is
+  // narrowed: a flank of 2^40 means "reach both ends", as in the context path.
+  const int64_t core = clamp_core(core_block_sites, S);
+  const int64_t flank = clamp_flank(flank_sites, S);
   const size_t slot_bytes = (size_t)core * kThreads * sizeof(float2);
   const int64_t capacity = (int64_t)((kNoAllocScratchBytes - kCounterBytes) / slot_bytes);
   if (capacity < 1) {
@@ -174,7 +180,7 @@ extern "C" int gsmc_run_fb_blockwise_device_noalloc(
     const int rc = scratch_address(v.device, &scratch);
     if (rc) return rc;
   }
-  const int64_t windows = (S + core_block_sites - 1) / core_block_sites;
+  const int64_t windows = window_count(S, core);
   const int64_t tiles = (n_pairs + kThreads - 1) / kThreads;
   if (windows * tiles > 0x7fffffff) return set_error(GSMC_E_INVALID, "too many tasks for one call");
   NoAllocArgs a;
@@ -190,9 +196,9 @@ extern "C" int gsmc_run_fb_blockwise_device_noalloc(
   a.counter = reinterpret_cast<int*>(scratch);
   a.slots = reinterpret_cast<float2*>(scratch + kCounterBytes);
   a.slot_rows = core;
-  a.n_sites = (int)S;
-  a.core = (int)std::min<int64_t>(core_block_sites, 0x7fffffff);
-  a.flank = (int)std::min<int64_t>(flank_sites, 0x7fffffff);
+  a.n_sites = S;
+  a.core = core;
+  a.flank = flank;
   a.n_pairs = (int)n_pairs;
   a.tiles = (int)tiles;
   a.n_tasks = (int)(windows * tiles);

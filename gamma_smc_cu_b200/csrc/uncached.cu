@@ -11,8 +11,9 @@
 // The 51 x 50 (u, v) grid -- 20,400 bytes, interleaved as float2 so a corner
 // is one 8-byte shared-memory read -- is staged once per CTA by a TMA bulk
 // copy (cp.async.bulk into shared memory, completion on an mbarrier).  The
-// wait for it is bounded: if the copy has not landed after a fixed number of
-// polls the CTA records an error and skips its pairs.  One thread per pair
+// wait for it is bounded: if the copy has not landed after a set number of
+// polls (UncachedArgs::wait_polls) the CTA records an error, waits (again
+// bounded) for the copy to finish and skips its pairs.  One thread per pair
 // walks all sites forward (states to a [S][P] float2 buffer) and back.
 //
 // The float arithmetic follows the reference expression by expression --
@@ -30,15 +31,33 @@ namespace {
 
 constexpr int kGridCells = kRows * kCols;            // 2550
 constexpr unsigned kFlowBytes = kGridCells * sizeof(float2);  // 20400, a multiple of 16
-constexpr long long kCopyPolls = 1ll << 24;            // bounded wait for the bulk copy
+// After giving up on the copy, a CTA still waits this many polls for it to
+// land before it exits, so that no bulk copy into its shared memory is in
+// flight when the CTA's shared memory is released.
+constexpr long long kDrainPolls = 1ll << 26;
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
 
+__device__ __forceinline__ uint32_t copy_landed(unsigned b) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(b)
+      : "memory");
+  return done;
+}
+
 // Stage the flow field into shared memory with one bulk copy; false if it did
-// not complete within the poll budget.
-__device__ bool stage_flow(float2* s_flow, uint64_t* bar, const float2* g_flow) {
+// not complete within `polls` polls of its mbarrier.  On false the CTA has
+// recorded the error in *error and, within a second bounded wait, let the
+// copy finish, so it may exit.
+__device__ bool stage_flow(float2* s_flow, uint64_t* bar, const float2* g_flow, long long polls,
+                           int* error) {
   const unsigned b = smem_addr(bar);
   if (threadIdx.x == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
@@ -55,16 +74,11 @@ __device__ bool stage_flow(float2* s_flow, uint64_t* bar, const float2* g_flow) 
         : "memory");
   }
   uint32_t done = 0;
-  for (long long i = 0; i < kCopyPolls && !done; ++i) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(b)
-        : "memory");
-  }
-  return done != 0;
+  for (long long i = 0; i < polls && !done; ++i) done = copy_landed(b);
+  if (done) return true;
+  if (threadIdx.x == 0) atomicExch(error, 1);
+  for (long long i = 0; i < kDrainPolls && !done; ++i) done = copy_landed(b);
+  return false;
 }
 
 // Bilinear (u, v) at (m, c) from the staged grid, the scan's interpolation.
@@ -189,10 +203,7 @@ template <bool CI>
 __global__ void __launch_bounds__(256) uncached_fb_kernel(const UncachedArgs a) {
   __shared__ __align__(16) float2 s_flow[kGridCells];
   __shared__ __align__(8) uint64_t bar;
-  if (!stage_flow(s_flow, &bar, a.flow)) {
-    if (threadIdx.x == 0) atomicExch(a.error, 1);
-    return;
-  }
+  if (!stage_flow(s_flow, &bar, a.flow, a.wait_polls, a.error)) return;
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.n_pairs) return;
   uncached_walk<CI>(a, s_flow, p, 0, 0, a.n_sites, a.n_sites, nullptr, nullptr, nullptr, nullptr);
@@ -207,10 +218,7 @@ template <bool CI>
 __global__ void __launch_bounds__(256) uncached_chunk_kernel(const UncachedArgs a, UncachedSpec sp) {
   __shared__ __align__(16) float2 s_flow[kGridCells];
   __shared__ __align__(8) uint64_t bar;
-  if (!stage_flow(s_flow, &bar, a.flow)) {
-    if (threadIdx.x == 0) atomicExch(a.error, 1);
-    return;
-  }
+  if (!stage_flow(s_flow, &bar, a.flow, a.wait_polls, a.error)) return;
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.n_pairs) return;
   const int k = blockIdx.y, K = sp.k_chunks, S = a.n_sites;
@@ -249,10 +257,7 @@ __global__ void __launch_bounds__(256) uncached_repair_kernel(const UncachedArgs
   if ((int)(blockIdx.x * blockDim.x) >= n) return;  // whole CTAs leave before staging
   __shared__ __align__(16) float2 s_flow[kGridCells];
   __shared__ __align__(8) uint64_t bar;
-  if (!stage_flow(s_flow, &bar, a.flow)) {
-    if (threadIdx.x == 0) atomicExch(a.error, 1);
-    return;
-  }
+  if (!stage_flow(s_flow, &bar, a.flow, a.wait_polls, a.error)) return;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t == 0) atomicAdd(sp.repaired_total, n);
   if (t >= n) return;

@@ -23,7 +23,11 @@ struct UncachedArgs {
   float* upper;
   int64_t ldo;
   int* error;              // set to 1 when a CTA's flow-field copy did not land
+  long long wait_polls;    // mbarrier polls a CTA waits for that copy before giving up
 };
+
+// Polls of the flow-field copy wait when no other budget is set.
+constexpr long long kDefaultCopyWaitPolls = 1ll << 24;
 
 // Exact speculative site chunks (as FwdSpec for the forward-only path): chunk
 // k of K decodes sites [S k / K, S (k+1) / K) with `burn_in` sites of burn-in

@@ -189,6 +189,7 @@ class TmrcaServer:
         self._done = []           # finished requests (for stats)
         self.counters = collections.Counter()
         self._redo_ex = None
+        self._redo_tasks = 0
         self._redo_stream = None
         self._thread = threading.Thread(target=self._loop, name="gsmc-serve", daemon=True)
         self._thread.start()
@@ -276,14 +277,21 @@ class TmrcaServer:
         """One query decoded as a single whole window (exact), on an executor
         made on first need: one-warp tiles, no chunking, a pool for at least
         one CTA of whole-window slots."""
-        if self._redo_ex is None:
+        # one whole window in one-warp tiles of 32 pairs: ceil(n_pairs / 32)
+        # tasks; the executor is sized for the largest redo so far
+        need = max(1, -(-job.n_pairs // 32))
+        if self._redo_ex is None or need > self._redo_tasks:
+            if self._redo_ex is not None:
+                self._redo_ex.close()
+                self._redo_ex = None
             slot = 4 * max(1, self.ctx.n_sites) * 32 * 8   # 4 one-warp tiles, float2 states
-            n_pairs = self.ctx.n_haps * (self.ctx.n_haps - 1) // 2
+            self._redo_tasks = max(1 << 8, need)
             self._redo_ex = Executor(self.ctx, tile_width=32, pairs_per_thread=1,
                                      core_block_sites=0, max_window_sites=self.ctx.n_sites,
-                                     max_tasks=max(1 << 12, -(-n_pairs // 32)),
+                                     max_tasks=self._redo_tasks,
                                      max_pool_bytes=max(1 << 30, slot), use_graph=False)
-            self._redo_stream = _new_stream(self.device)
+            if self._redo_stream is None:
+                self._redo_stream = _new_stream(self.device)
         b = DeviceBatch(Layout([job]), self.device)
         b.launch(self._redo_ex, self._redo_stream)
         return b.to_host()[0]

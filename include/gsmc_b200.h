@@ -214,8 +214,12 @@ int gsmc_run_fb_blockwise_device(gsmc_ctx* ctx, const int32_t* d_pair_i,
  * the library until exit; core_block_sites above 131,071 (one CTA slot no
  * longer fits) is rejected with GSMC_E_INVALID.  All calls share that array:
  * calls that overlap on the GPU race and must be serialised by the caller.
- * The first call on each device looks the array's address up; make it before
- * any stream capture.  No counterpart in the reference.
+ * The first call on each device looks the array's address up and keeps it
+ * for the life of the process; make it before any stream capture, and do not
+ * use this entry point on a device after cudaDeviceReset (the kept address
+ * would then be stale).  core_block_sites and flank_sites are clamped to the
+ * sequence length in int64, as the context path does.  No counterpart in the
+ * reference.
  */
 int gsmc_run_fb_blockwise_device_noalloc(gsmc_ctx* ctx, const int32_t* d_pair_i,
                                          const int32_t* d_pair_j, int64_t n_pairs,
@@ -399,6 +403,19 @@ int gsmc_flow_fb(const uint8_t* G, int64_t n_haps, int64_t n_sites, const double
                  const int32_t* pair_i, const int32_t* pair_j, int64_t n_pairs, double Ne,
                  double mu, double rho, const char* flow_field_path, int flags, float* mean,
                  float* lower, float* upper);
+
+/*
+ * Poll budget of the uncached kernels' wait for their shared-memory copy of
+ * the flow field (default 2^24 mbarrier polls, process-wide, read at each
+ * gsmc_flow_fb call).  A CTA whose copy has not landed within the budget
+ * sets an error flag, waits (bounded) for the copy to finish and skips its
+ * pairs; the call then returns GSMC_E_TIMEOUT and the next call runs
+ * normally.  A budget of 0 gives up at once, which tests use to exercise that
+ * path.  *previous (if not NULL) receives the old budget.  No reference
+ * counterpart (the reference waits without a limit and prints launch errors,
+ * src/kernels/gamma_smc_flow.cu:365-369).
+ */
+int gsmc_set_copy_wait_polls(int64_t polls, int64_t* previous);
 
 /*
  * Bit-pack genotypes on the device: packed[h * n_words + w] bit b =

@@ -106,3 +106,28 @@ def test_flow_fb_speculative_site_chunks_are_exact(oracle, flow_field, ref_core,
             ref = ref_core.gamma_smc_flow_fb(G, pos, pairs, 1e4, 1.25e-8, 1e-8, flow_field, False)
             for k in KEYS:
                 assert np.array_equal(got[k], ref[k]), k
+
+
+def test_flow_fb_copy_wait_runs_out_then_recovers(small_data, flow_field):
+    """A poll budget of 0 makes every CTA give up on its flow-field copy at
+    once: the call reports GSMC_E_TIMEOUT (the CTAs still let their copies
+    finish before exiting), and the next call on the same device, with the
+    default budget back, is exact again."""
+    import ctypes
+    from gamma_smc_cu_b200 import _lib
+    L = _lib.load()
+    G, pos = small_data
+    pairs = [(i, j) for i in range(12) for j in range(i)]
+    want = G200.gamma_smc_flow_fb(G, pos, pairs, flow_field_path=flow_field, mean_only=True)
+    prev = ctypes.c_int64()
+    _lib.check(L.gsmc_set_copy_wait_polls(0, ctypes.byref(prev)))
+    try:
+        with pytest.raises(_lib.GsmcError, match="did not complete"):
+            G200.gamma_smc_flow_fb(G, pos, pairs, flow_field_path=flow_field, mean_only=True)
+    finally:
+        _lib.check(L.gsmc_set_copy_wait_polls(prev.value, None))
+    assert prev.value == 1 << 24
+    got = G200.gamma_smc_flow_fb(G, pos, pairs, flow_field_path=flow_field, mean_only=True)
+    assert np.array_equal(got["mean"], want["mean"])
+    with pytest.raises(ValueError, match="non-negative"):
+        _lib.check(L.gsmc_set_copy_wait_polls(-1, None))

@@ -1,0 +1,82 @@
+"""Window arithmetic of the blockwise decoders, on the CPU.
+
+csrc/windows.h holds the one definition of the blockwise windows (core
+[cs, ce) padded by flank sites on both sides, clamped to the sequence;
+src/bindings.cpp:2517-2534 in the reference) that the context planner and the
+allocation-free kernel share.  Here it is compiled as plain C++ and compared,
+for extreme int64 core and flank values, against the same definition in
+unbounded Python integers: every bound must lie in [0, n_sites], so no kernel
+can index outside the sequence whatever the caller passes.
+"""
+import os
+import subprocess
+
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(os.path.dirname(HERE), "gamma_smc_cu_b200", "csrc")
+
+DRIVER = r"""
+#include <cstdio>
+#include "windows.h"
+int main() {
+  long long S, core, flank;
+  while (std::scanf("%lld %lld %lld", &S, &core, &flank) == 3) {
+    const long long n = gsmc::window_count(S, core);
+    std::printf("%lld", n);
+    const long long ws[3] = {0, n / 2, n - 1};
+    for (long long w : ws) {
+      if (n == 0) break;
+      const gsmc::WindowBounds b = gsmc::window_bounds(w, S, core, flank);
+      std::printf(" %lld %lld %lld %lld %lld", w, (long long)b.ps, (long long)b.cs,
+                  (long long)b.ce, (long long)b.pe);
+    }
+    std::printf("\n");
+  }
+  return 0;
+}
+"""
+
+INT64_MAX = 2**63 - 1
+
+
+def _expected(S, core, flank, w):
+    cs = w * core
+    ce = min(S, cs + core)
+    return max(0, cs - flank), cs, ce, min(S, ce + flank)
+
+
+@pytest.fixture(scope="module")
+def driver(tmp_path_factory):
+    d = tmp_path_factory.mktemp("windows")
+    src = d / "drv.cpp"
+    src.write_text(DRIVER)
+    exe = d / "drv"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", CSRC, str(src), "-o", str(exe)], check=True)
+    return str(exe)
+
+
+def test_window_bounds_stay_in_the_sequence(driver):
+    sizes = [1, 2, 7, 1000, 400_000, 2**31 - 2]
+    cores = [1, 3, 1024, 32_768, 2**31 - 1, 2**40, INT64_MAX]
+    flanks = [0, 1, 2048, 2**31 - 1, 2**31, 2**40, INT64_MAX]
+    cases = [(S, c, f) for S in sizes for c in cores for f in flanks
+             if (S + c - 1) // c <= 10**9]  # keep the window counts printable
+    inp = "".join(f"{S} {c} {f}\n" for S, c, f in cases)
+    out = subprocess.run([driver], input=inp, capture_output=True, text=True, check=True).stdout
+    lines = out.strip().splitlines()
+    assert len(lines) == len(cases)
+    for (S, core, flank), line in zip(cases, lines):
+        v = [int(x) for x in line.split()]
+        n = (S + core - 1) // core
+        assert v[0] == n, (S, core, flank)
+        for k in range(1, len(v), 5):
+            w, ps, cs, ce, pe = v[k:k + 5]
+            assert (ps, cs, ce, pe) == _expected(S, core, flank, w), (S, core, flank, w)
+            assert 0 <= ps <= cs < ce <= pe <= S, (S, core, flank, w)
+
+
+def test_zero_sites_has_no_window(driver):
+    out = subprocess.run([driver], input="0 5 3\n", capture_output=True, text=True,
+                         check=True).stdout
+    assert out.strip() == "0"

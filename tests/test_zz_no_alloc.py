@@ -81,6 +81,12 @@ def test_noalloc_matches_allocating_entry_point_twice():
     want = _run(L.gsmc_run_fb_blockwise_device, ctx, pi, pj, S, S, 0)
     _assert_close(a, want)
     _assert_close(b, want)
+    # flanks (and cores) far beyond the sequence reach both ends, as they do in
+    # the context path: both entry points clamp them to the sequence in int64
+    for core, flank in ((700, 1 << 40), (1 << 40, 1 << 40)):
+        got = _run(L.gsmc_run_fb_blockwise_device_noalloc, ctx, pi, pj, S, core, flank)
+        want = _run(L.gsmc_run_fb_blockwise_device, ctx, pi, pj, S, core, flank)
+        _assert_close(got, want)
 
 
 def test_noalloc_rejects_core_beyond_scratch():

@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--no-summary", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own GPU build on the same jobs")
     ap.add_argument("--no-stress", action="store_true",
                     help="skip the 2,000-haplotype x 1,000,000-pair streamed run")
     ap.add_argument("--plain-jobs", type=int, default=48,
@@ -195,12 +197,15 @@ def run_reference(args, rank, world):
     mu, rho = _estimate_scaled_params(G, pos, 1.25e-8, 1e-8, 1e4)
     threads = os.cpu_count() or 1
     O.tables_for(DEFAULT_FLOW_FIELD, 1e4, mu, rho)
-    probe = pairs[:max(8, threads)]
+    # A step is a bounded pair sample of the job: at least 4,096 pairs (enough
+    # work per thread that every host core stays busy to the end) and at least
+    # ~8 s of CPU work, sized from a 256-pair probe.
+    probe = pairs[:min(len(pairs), 256)]
     t0 = time.perf_counter()
     O.run_fb_blockwise(G, pos, [tuple(p) for p in probe], 1e4, mu, rho, DEFAULT_FLOW_FIELD,
                        core, flank, True, False, threads)
     dt = time.perf_counter() - t0
-    n_sample = int(min(len(pairs), max(len(probe), len(probe) * 4.0 / max(dt, 1e-3))))
+    n_sample = int(min(len(pairs), max(4096, len(probe) * 8.0 / max(dt, 1e-3))))
     sample = [tuple(p) for p in pairs[:n_sample]]
     for _ in range(args.warmup):
         O.run_fb_blockwise(G, pos, sample, 1e4, mu, rho, DEFAULT_FLOW_FIELD, core, flank, True,
@@ -307,8 +312,10 @@ def main():
     value = P * S * world / (t_ms / 1e3 / args.steps)
     hbm, peak_kind = peaks()
     achieved = psites.value * BYTES_MEAN_ONLY / (kms.value / 1e3) / 1e9
-    sample = out[::max(1, S // 64), ::max(1, P // 64)]
-    assert bool(torch.isfinite(sample).all()) and bool((sample > 0).all()), "bad posterior"
+    # parity sample: 64 seeded-random pair columns of the timed output, all
+    # 400,000 sites, checked against the oracle after the GPU work
+    cols = np.sort(np.random.default_rng(11).choice(P, size=min(64, P), replace=False))
+    ours_cols = out[:, torch.from_numpy(cols).to(dev)].cpu().numpy()
     del out
     ctx.release_scratch()
     torch.cuda.empty_cache()
@@ -339,9 +346,25 @@ def main():
     e2e = None
     if not args.no_e2e:
         e2e = run_e2e(G, pos, pairs, core, flank, args.e2e_steps)
+    ref_gpu = None
+    if args.workload == "chrom" and rank == 0 and not args.no_reference_gpu:
+        ref_gpu = run_reference_gpu(G, pos, pairs, core, flank, mu, rho, cols, ours_cols,
+                                    e2e, full)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(G, pos, pairs, core, flank, mu, rho)
+    parity = None
+    if rank == 0:
+        parity = {"chrom": oracle_parity(G, pos, pairs[cols], mu, rho, core, flank,
+                                         {"mean": ours_cols})}
+        if full is not None:
+            parity["full_posterior"] = full.pop("parity")
+        if stress is not None:
+            parity["stream_stress"] = stress.pop("parity")
+        parity["exact"] = all(v["exact"] for v in parity.values())
+        parity["max_rel"] = max(v["max_rel"] for k, v in parity.items() if isinstance(v, dict))
+        parity["pairs_checked"] = sum(v["pairs_checked"] for v in parity.values()
+                                      if isinstance(v, dict))
 
     if rank == 0:
         line = {
@@ -365,6 +388,8 @@ def main():
             "clocks": clk.summary(),
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "parity": parity,
+            "reference_gpu": ref_gpu,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -432,17 +457,165 @@ def run_full_posterior(G, pos, pairs, steps, warmup, dev, n_sites=50_000):
     achieved = psites / steps_ * BYTES_FULL_POSTERIOR / (kms / 1e3) / 1e9
     recon = (outs[1][::997, ::61] / outs[2][::997, ::61]) * 2e4
     ok = bool(torch.allclose(recon, outs[0][::997, ::61], rtol=1e-4, atol=1e-2))
+    cols = np.sort(np.random.default_rng(12).choice(P, size=min(64, P), replace=False))
+    ct = torch.from_numpy(cols).to(dev)
+    got = {k: o[:, ct].cpu().numpy() for k, o in zip(("mean", "posterior_alpha",
+                                                       "posterior_beta"), outs)}
     del outs
+    shape = ctx.scan_shape()
+    spec = ctx.spec_stats()
     ctx.close()
     torch.cuda.empty_cache()
+    parity = oracle_parity(Gs, ps, pairs[cols], mu, rho, core, 2048, got, posterior=True)
     return {"workload": f"chrom 50k-site slice: 356 haps x {S} sites x {P} pairs, mean+alpha+beta",
-            "core_block_sites": int(core), "flank_sites": 2048,
+            "core_block_sites": int(core), "flank_sites": 2048, "scan_shape": shape,
+            "speculative": spec, "parity": parity, "mu": mu, "rho": rho,
             "value": P * S / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
             "gpu_launches": int(launches), "posterior_consistent": ok,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "peak_kind": kind,
                          "bytes_per_pair_site": BYTES_FULL_POSTERIOR, "traffic": None,
                          "kernel_ms_per_step": kms}}
+
+
+def oracle_parity(G, pos, pairs, mu, rho, core, flank, got, posterior=False):
+    """Bitwise comparison of sampled pair columns (``got``: output name ->
+    [n_sites, len(pairs)] float32 from the GPU run) with the CPU oracle run
+    blockwise on the same pairs, core and flank.  The oracle is only the
+    checker here and runs outside every timed region."""
+    from oracle import oracle as O
+    from gamma_smc_cu_b200._core import DEFAULT_FLOW_FIELD
+    t0 = time.perf_counter()
+    want = O.run_fb_blockwise(G, pos, [(int(i), int(j)) for i, j in pairs], 1e4, mu, rho,
+                              DEFAULT_FLOW_FIELD, int(core), int(flank), True, posterior,
+                              os.cpu_count() or 1)
+    exact, mr = True, 0.0
+    for k, g in got.items():
+        w = want[k][:g.shape[0]]
+        exact &= bool(np.array_equal(np.ascontiguousarray(g).view(np.uint32),
+                                     np.ascontiguousarray(w).view(np.uint32)))
+        mr = max(mr, _max_rel(g, w))
+    return {"pairs_checked": int(len(pairs)), "sites": int(next(iter(got.values())).shape[0]),
+            "core_block_sites": int(core), "flank_sites": int(flank), "outputs": sorted(got),
+            "exact": exact, "max_rel": mr, "oracle_seconds": time.perf_counter() - t0}
+
+
+def _reference_core():
+    """The reference's own _core module, compiled from its sources for sm_100a
+    into oracle/_ref by the oracle recipe, or None when it was not built."""
+    import importlib.util
+    from oracle import oracle as O
+    path = O.ref_core_path()
+    if path is None:
+        return None
+    spec = importlib.util.spec_from_file_location("_core", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _cuda_kernel_ms(fn):
+    """Run fn() once with CUDA kernel activity recorded (CUPTI, through
+    torch.profiler; no replay): (fn's result, {kernel name: total ms})."""
+    from torch.profiler import ProfilerActivity, profile
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        r = fn()
+    ms = {}
+    for e in prof.key_averages():
+        t = getattr(e, "device_time_total", None)
+        if t is None:
+            t = getattr(e, "cuda_time_total", 0.0)
+        if t:
+            ms[e.key] = ms.get(e.key, 0.0) + t / 1e3
+    return r, ms
+
+
+def _scan_kernel_ms(ms):
+    """Total ms of the reference's cached forward/backward kernels."""
+    return sum(v for k, v in ms.items() if "gamma_smc_cached" in k or "precompute_xor" in k)
+
+
+def run_reference_gpu(G, pos, pairs, core, flank, mu, rho, cols, ours_cols, e2e, full,
+                      kernel_pairs=8192):
+    """Informational: the reference's own GPU build (its pybind11 _core from
+    the reference sources, compiled for sm_100a) on the same box and jobs,
+    through its public FlowContext API with host outputs, timed by wall clock
+    like ``e2e``: the chromosome job (FlowContext + run_fb_blockwise) and the
+    50k-site full-posterior slice (FlowContext + run_fb).  Reports seconds,
+    pair-sites/s, the speed-up of this build's same call, and whether the
+    sampled columns are bit-equal to this build's."""
+    import psutil
+    ref = _reference_core()
+    if ref is None:
+        return {"unavailable": "the reference _core was not built into oracle/_ref"}
+    from gamma_smc_cu_b200._core import DEFAULT_FLOW_FIELD
+    out = {"build": "reference sources, nvcc 12.9 -gencode arch=compute_100a,code=sm_100a "
+                    "(its own CMake targets sm_80)"}
+    S, P = G.shape[1], len(pairs)
+    sites = S
+    avail = psutil.virtual_memory().available
+    if 4.0 * S * P > 0.6 * avail:
+        sites = int(0.6 * avail / (4.0 * P))
+    Gs, ps = np.ascontiguousarray(G[:, :sites]), np.ascontiguousarray(pos[:sites])
+    plist = [tuple(p) for p in pairs.tolist()]
+    t0 = time.perf_counter()
+    ctx = ref.FlowContext(Gs, ps, 1e4, mu, rho, DEFAULT_FLOW_FIELD, 0)
+    r = ref.FlowContext.run_fb_blockwise(ctx, plist, int(core), int(flank), -1, 1, True, False)
+    t = time.perf_counter() - t0
+    m = r["mean"]
+    eq = bool(np.array_equal(np.ascontiguousarray(m[:, cols]).view(np.uint32),
+                             np.ascontiguousarray(ours_cols[:sites]).view(np.uint32)))
+    del r, m, ctx
+    job = {"workload": f"chrom: 356 haps x {sites} sites x {P} pairs, blockwise core {core} / "
+                       f"flank {flank}, mean_only, host outputs", "seconds": t,
+           "value": P * sites / t, "unit": UNIT, "sampled_columns_bit_equal": eq}
+    if e2e is not None and e2e.get("sites") == sites:
+        job["ours_e2e_seconds"] = e2e["seconds_per_step"]
+        job["speedup_e2e"] = t / e2e["seconds_per_step"]
+    # the reference's kernels alone, on 8,192 of the pairs (CUPTI activity
+    # records of one run, taken separately from the wall-clock run above)
+    sub = plist[:kernel_pairs]
+    ctx = ref.FlowContext(Gs, ps, 1e4, mu, rho, DEFAULT_FLOW_FIELD, 0)
+    r, ms = _cuda_kernel_ms(lambda: ref.FlowContext.run_fb_blockwise(
+        ctx, sub, int(core), int(flank), -1, 1, True, False))
+    del r, ctx
+    kms = _scan_kernel_ms(ms)
+    job["kernels"] = {"pairs": len(sub), "scan_kernel_ms": kms,
+                      "kernel_pair_sites_per_s": len(sub) * sites / (kms / 1e3) if kms else None,
+                      "by_kernel_ms": {k: v for k, v in sorted(ms.items(), key=lambda kv: -kv[1])[:6]}}
+    out["chrom"] = job
+    if full is not None:
+        n = 50_000
+        Gs, ps = np.ascontiguousarray(G[:, :n]), np.ascontiguousarray(pos[:n])
+        fmu, frho = full["mu"], full["rho"]
+        t0 = time.perf_counter()
+        ctx = ref.FlowContext(Gs, ps, 1e4, fmu, frho, DEFAULT_FLOW_FIELD, 0)
+        r = ref.FlowContext.run_fb(ctx, plist, True, True)
+        t = time.perf_counter() - t0
+        want = {k: r[k][:, cols] for k in ("mean", "posterior_alpha", "posterior_beta")}
+        del r
+        r, ms = _cuda_kernel_ms(lambda: ref.FlowContext.run_fb(ctx, plist, True, True))
+        del r, ctx
+        kms = _scan_kernel_ms(ms)
+        from gamma_smc_cu_b200 import _core
+        t0 = time.perf_counter()
+        ctx = _core.FlowContext(Gs, ps, 1e4, fmu, frho, DEFAULT_FLOW_FIELD, 0)
+        o = ctx.run_fb(plist, mean_only=True, return_posterior=True)
+        t_ours = time.perf_counter() - t0
+        ctx.close()
+        eq = all(np.array_equal(np.ascontiguousarray(o[k][:, cols]).view(np.uint32),
+                                np.ascontiguousarray(w).view(np.uint32))
+                 for k, w in want.items())
+        del o
+        out["full_posterior"] = {
+            "workload": f"chrom 50k-site slice: {n} sites x {P} pairs, run_fb mean + alpha + "
+                        "beta, host outputs", "seconds": t, "value": P * n / t, "unit": UNIT,
+            "ours_seconds": t_ours, "speedup": t / t_ours, "sampled_columns_bit_equal": eq,
+            "scan_kernel_ms": kms,
+            "kernel_pair_sites_per_s": P * n / (kms / 1e3) if kms else None,
+            "ours_kernel_ms": full["roofline"]["kernel_ms_per_step"],
+            "kernel_speedup": kms / full["roofline"]["kernel_ms_per_step"] if kms else None}
+    return out
 
 
 def _max_rel(a, b):
@@ -685,6 +858,10 @@ def run_stream_stress(core=8192, flank=2048):
     mu, rho = _estimate_scaled_params(G, pos, 1.25e-8, 1e-8, 1e4)
     L = _lib.load()
     stats = {"units": 0, "bytes": 0, "bad": 0}
+    # parity sample: 16 of the million pairs, every site, collected from the
+    # streamed units and checked against the oracle afterwards
+    pick = np.sort(np.random.default_rng(13).choice(P, size=16, replace=False))
+    kept = np.full((S, len(pick)), np.nan, np.float32)
 
     def sink(s0, s1, p0, p1, outs):
         m = outs["mean"]
@@ -692,6 +869,9 @@ def run_stream_stress(core=8192, flank=2048):
         stats["bytes"] += m.shape[0] * m.shape[1] * 4
         probe = m[:: max(1, m.shape[0] // 4), :: max(1, m.shape[1] // 8)]
         stats["bad"] += int((~np.isfinite(probe) | (probe <= 0)).sum())
+        sel = np.nonzero((pick >= p0) & (pick < p1))[0]
+        if sel.size:
+            kept[s0:s1, sel] = m[:, pick[sel] - p0]
         return False
 
     t0 = time.perf_counter()
@@ -705,8 +885,10 @@ def run_stream_stress(core=8192, flank=2048):
     _lib.check(L.gsmc_ctx_timing_read(ctx.handle, ctypes.byref(kms), ctypes.byref(launches),
                                       ctypes.byref(psites)))
     ctx.close()
+    parity = oracle_parity(G, pos, pairs[pick], mu, rho, core, flank, {"mean": kept})
     total = float(S) * P
-    return {"workload": "cohort 2,000 haps x 200,000 sites x 1,000,000 random pairs, blockwise "
+    return {"parity": parity,
+            "workload": "cohort 2,000 haps x 200,000 sites x 1,000,000 random pairs, blockwise "
                         f"core {core} / flank {flank}, mean_only, streamed to a host sink",
             "pair_sites": total, "seconds": wall, "value": total / wall, "unit": UNIT,
             "d2h_gb_per_s": stats["bytes"] / wall / 1e9, "units": stats["units"],

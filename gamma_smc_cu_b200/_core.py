@@ -352,6 +352,14 @@ class FlowContext:
         check(_lib.load().gsmc_ctx_scan_shape(self._h, ctypes.byref(w), ctypes.byref(k)))
         return int(w.value), int(k.value)
 
+    def spec_stats(self):
+        """(launches cut into exact speculative site chunks, (window, pair)s
+        decoded again whole after a failed boundary check) of this context so
+        far; no reference counterpart."""
+        a, r = ctypes.c_int64(), ctypes.c_int64()
+        check(_lib.load().gsmc_ctx_spec_stats(self._h, ctypes.byref(a), ctypes.byref(r)))
+        return int(a.value), int(r.value)
+
     def table_layer(self, table, layer):
         """Debug: (m_grid, c_grid) [51, 50] of scan table 0..4 at a layer."""
         buf = np.empty(2 * 2550, np.float32)

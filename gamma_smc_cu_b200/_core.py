@@ -104,6 +104,13 @@ def gamma_smc_flow_fb(G, positions, pairs, Ne=10000.0, mu=1.25e-8, rho=1e-8,
     return out
 
 
+def free_cached_tables():
+    """Free the scan-table sets no live context holds (the most recently
+    released set of each device otherwise stays resident for the next context
+    with the same parameters); no reference counterpart."""
+    check(_lib.load().gsmc_free_cached_tables())
+
+
 def _split_pairs(pairs):
     """List of (i, j) (or an (P, 2) array) -> two contiguous int32 arrays."""
     if isinstance(pairs, np.ndarray):
@@ -128,8 +135,13 @@ class FlowContext:
     """
 
     def __init__(self, G, positions, Ne=10000.0, mu=1.25e-8, rho=1e-8,
-                 flow_field_path=DEFAULT_FLOW_FIELD, cache_steps=0):
+                 flow_field_path=DEFAULT_FLOW_FIELD, cache_steps=0, table_build="host_fp32"):
+        """``table_build`` (no reference counterpart): "host_fp32" builds the
+        scan tables on the host exactly as the reference does (bit-identical
+        results); "gpu_fp64" builds them on the GPU in float64."""
         L = _lib.load()
+        if table_build not in ("host_fp32", "gpu_fp64"):
+            raise ValueError("table_build must be 'host_fp32' or 'gpu_fp64'")
         G = np.ascontiguousarray(G, dtype=np.uint8)
         positions = np.ascontiguousarray(positions, dtype=np.float64)
         if G.ndim != 2:
@@ -138,10 +150,11 @@ class FlowContext:
         if positions.ndim != 1 or positions.shape[0] != S:
             raise ValueError("positions length must match the number of sites in G")
         h = ctypes.c_void_p()
-        check(L.gsmc_ctx_create(ptr(G, _lib.c_u8p), n, S, ptr(positions, _lib.c_f64p),
-                                float(Ne), float(mu), float(rho),
-                                os.fsencode(str(flow_field_path)), int(cache_steps),
-                                ctypes.byref(h)))
+        flags = _lib.GSMC_TABLES_GPU_F64 if table_build == "gpu_fp64" else 0
+        check(L.gsmc_ctx_create_ex(ptr(G, _lib.c_u8p), n, S, ptr(positions, _lib.c_f64p),
+                                   float(Ne), float(mu), float(rho),
+                                   os.fsencode(str(flow_field_path)), int(cache_steps), flags,
+                                   ctypes.byref(h)))
         self._h = h
         self._n = n
         self._S = S
@@ -359,6 +372,14 @@ class FlowContext:
         a, r = ctypes.c_int64(), ctypes.c_int64()
         check(_lib.load().gsmc_ctx_spec_stats(self._h, ctypes.byref(a), ctypes.byref(r)))
         return int(a.value), int(r.value)
+
+    def tables_info(self):
+        """{"build_seconds": build + upload of this context's scan tables (0.0
+        when it reused a resident set), "reused": bool}; no reference
+        counterpart."""
+        secs, reused = ctypes.c_double(), ctypes.c_int()
+        check(_lib.load().gsmc_ctx_tables_info(self._h, ctypes.byref(secs), ctypes.byref(reused)))
+        return {"build_seconds": float(secs.value), "reused": bool(reused.value)}
 
     def table_layer(self, table, layer):
         """Debug: (m_grid, c_grid) [51, 50] of scan table 0..4 at a layer."""

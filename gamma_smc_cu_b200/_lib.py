@@ -25,6 +25,8 @@ GSMC_E_TIMEOUT = -5
 GSMC_CI = 1
 GSMC_POSTERIOR = 2
 
+GSMC_TABLES_GPU_F64 = 1
+
 c_i64 = ctypes.c_int64
 c_u64p = ctypes.POINTER(ctypes.c_uint64)
 c_i64p = ctypes.POINTER(ctypes.c_int64)
@@ -82,6 +84,9 @@ SIGNATURES = {
     "gsmc_get_device": (c_int, [c_intp]),
     "gsmc_ctx_create": (c_int, [c_u8p, c_i64, c_i64, c_f64p, ctypes.c_double, ctypes.c_double,
                                 ctypes.c_double, ctypes.c_char_p, c_int, ctypes.POINTER(c_vp)]),
+    "gsmc_ctx_create_ex": (c_int, [c_u8p, c_i64, c_i64, c_f64p, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_char_p, c_int, c_int,
+                                   ctypes.POINTER(c_vp)]),
     "gsmc_ctx_destroy": (c_int, [c_vp]),
     "gsmc_ctx_info": (c_int, [c_vp, c_intp, c_i64p, c_i64p]),
     "gsmc_run_fb": (c_int, [c_vp, c_i32p, c_i32p, c_i64, c_int, c_f32p, c_f32p, c_f32p,
@@ -126,6 +131,8 @@ SIGNATURES = {
     "gsmc_ctx_timing_read": (c_int, [c_vp, ctypes.POINTER(ctypes.c_double), c_i64p,
                                      ctypes.POINTER(ctypes.c_double)]),
     "gsmc_set_copy_wait_polls": (c_int, [c_i64, c_i64p]),
+    "gsmc_ctx_tables_info": (c_int, [c_vp, ctypes.POINTER(ctypes.c_double), c_intp]),
+    "gsmc_free_cached_tables": (c_int, []),
     "gsmc_bitpack": (c_int, [c_u8p, c_i64, c_i64, c_u64p]),
     "gsmc_unpack": (c_int, [c_u64p, c_i64, c_i64, c_u8p]),
     "gsmc_ctx_table_layer": (c_int, [c_vp, c_int, c_int, c_f32p]),

@@ -20,10 +20,11 @@ LIBDIR = os.path.join(HERE, "lib")
 OBJDIR = os.path.join(HERE, "_build")
 LIB = os.path.join(LIBDIR, "libgsmc_b200.so")
 
-CUDA_SOURCES = ["scan.cu", "capi.cu", "hostcopy.cu", "exec.cu", "fwd.cu", "flowgen.cu", "uncached.cu", "noalloc.cu"]
+CUDA_SOURCES = ["scan.cu", "capi.cu", "hostcopy.cu", "exec.cu", "fwd.cu", "flowgen.cu", "uncached.cu",
+                "noalloc.cu", "tables_gpu.cu"]
 CXX_SOURCES = ["tables.cpp"]
 HEADERS = ["scan.h", "scan_device.cuh", "tables.h", "hostcopy.h", "ctx_view.h", "fwd.h", "flowgen.h", "uncached.h",
-           "windows.h"]
+           "windows.h", "tables_gpu.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",

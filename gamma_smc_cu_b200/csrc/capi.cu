@@ -4,6 +4,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <condition_variable>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -23,6 +25,7 @@
 #include "hostcopy.h"
 #include "scan.h"
 #include "tables.h"
+#include "tables_gpu.h"
 #include "uncached.h"
 #include "windows.h"
 
@@ -60,10 +63,18 @@ int fail(int code, const char* fmt, ...) {
   } while (0)
 
 // ------------------------------------------------------------ table sets --
-// One resident set of scan tables per (device, flow field, Ne, mu, rho, L),
-// shared by every context with those parameters and freed with the last one.
-// (The reference keeps a single process-global set and frees it under live
-// contexts when the parameters change, src/bindings.cpp:2016-2041.)
+// One resident set of scan tables per (device, flow field, Ne, mu, rho, L,
+// build), shared by every context with those parameters.  (The reference
+// keeps a single process-global set and frees it under live contexts when the
+// parameters change, src/bindings.cpp:2016-2041.)
+//
+// A set is built outside the global lock: the first context to ask for a key
+// inserts an in-progress entry and builds; others asking for the same key
+// wait for it, and other keys proceed meanwhile.  When its last context
+// closes, a set is parked: the most recently released set of each device
+// stays resident for the next context with the same parameters (as the
+// reference's process-wide cache does), and parking a newer set frees the
+// older one.  gsmc_free_cached_tables frees parked sets.
 struct TableSet {
   int device = 0;
   int L = 0;
@@ -75,62 +86,20 @@ struct TableSet {
   uint4* hom_half = nullptr;        // [L][2450] half patches
   std::mutex half_mu;
   int refs = 0;
+  bool ready = false;       // build finished (status says how)
+  int status = GSMC_OK;
+  std::string error;
+  double build_seconds = 0.0;  // build + upload
 };
 
-using TableKey = std::tuple<int, std::string, float, float, float, int>;
+// (device, flow field, Ne, mu, rho, layers, float64 GPU build)
+using TableKey = std::tuple<int, std::string, float, float, float, int, bool>;
 std::mutex g_tables_mu;
+std::condition_variable g_tables_cv;
 std::map<TableKey, TableSet*> g_tables;
+std::map<int, TableSet*> g_parked;  // device -> its released, still resident set
 
-int acquire_tables(int device, const char* ff_path, float ne, float mu, float rho, int L,
-                   TableSet** out) {
-  std::lock_guard<std::mutex> lock(g_tables_mu);
-  TableKey key{device, std::string(ff_path), ne, mu, rho, L};
-  auto it = g_tables.find(key);
-  if (it != g_tables.end()) {
-    it->second->refs++;
-    *out = it->second;
-    return GSMC_OK;
-  }
-  FlowField ff;
-  char err[512];
-  if (load_flow_field(ff_path, &ff, err, sizeof(err)) != 0) return fail(GSMC_E_IO, "%s", err);
-  float srho, smu;
-  scaled_rates(ne, mu, rho, &srho, &smu);
-  HostLayers layers;
-  build_layers(ff, L, srho, smu, 0, &layers);
-  std::vector<float> site, chunk;
-  build_scan_layout(layers, &site, &chunk, 0);
-  auto keep_hom = [&](TableSet* t) {
-    t->hom_m = std::move(layers.t[kHomMean]);
-    t->hom_c = std::move(layers.t[kHomCv]);
-  };
-  auto ts = std::make_unique<TableSet>();
-  ts->device = device;
-  ts->L = L;
-  CUDA_TRY(cudaMalloc(&ts->site, site.size() * sizeof(float)));
-  if (cudaMalloc(&ts->chunk, chunk.size() * sizeof(float)) != cudaSuccess) {
-    cudaFree(ts->site);
-    return fail(GSMC_E_CUDA, "CUDA error: cudaMalloc of the chunk table failed");
-  }
-  CUDA_TRY(cudaMemcpy(ts->site, site.data(), site.size() * sizeof(float), cudaMemcpyHostToDevice));
-  CUDA_TRY(cudaMemcpy(ts->chunk, chunk.data(), chunk.size() * sizeof(float),
-                      cudaMemcpyHostToDevice));
-  keep_hom(ts.get());
-  ts->refs = 1;
-  *out = ts.get();
-  g_tables[key] = ts.release();
-  return GSMC_OK;
-}
-
-void release_tables(TableSet* ts) {
-  if (!ts) return;
-  std::lock_guard<std::mutex> lock(g_tables_mu);
-  if (--ts->refs > 0) return;
-  for (auto it = g_tables.begin(); it != g_tables.end(); ++it)
-    if (it->second == ts) {
-      g_tables.erase(it);
-      break;
-    }
+void free_table_set(TableSet* ts) {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(ts->device);
@@ -139,6 +108,148 @@ void release_tables(TableSet* ts) {
   cudaFree(ts->hom_half);
   cudaSetDevice(prev);
   delete ts;
+}
+
+void erase_key_of(TableSet* ts) {
+  for (auto it = g_tables.begin(); it != g_tables.end(); ++it)
+    if (it->second == ts) {
+      g_tables.erase(it);
+      return;
+    }
+}
+
+// Drop one reference (g_tables_mu held).  A built set whose last reference
+// goes is parked; the set it displaces, or a set whose build failed, is freed.
+void drop_ref_locked(TableSet* ts) {
+  if (--ts->refs > 0) return;
+  if (ts->status != GSMC_OK) {
+    free_table_set(ts);  // already out of the map
+    return;
+  }
+  auto it = g_parked.find(ts->device);
+  if (it != g_parked.end() && it->second != ts) {
+    TableSet* old = it->second;
+    erase_key_of(old);
+    free_table_set(old);
+  }
+  g_parked[ts->device] = ts;
+}
+
+// Float64 build on the device (tables_gpu.cu) of one set, into ts.
+int build_table_set_f64(const FlowField& ff, double ne, double mu, double rho, int L, TableSet* ts,
+                        std::string* err) {
+  int prev = 0;
+  cudaGetDevice(&prev);
+  const size_t site_bytes = (size_t)kScanTables * L * kPatches * 8 * sizeof(float);
+  const size_t chunk_bytes = (size_t)kPatches * 8 * sizeof(float);
+  cudaError_t e = cudaSetDevice(ts->device);
+  if (e == cudaSuccess) e = cudaMalloc(&ts->site, site_bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&ts->chunk, chunk_bytes);
+  int rc = GSMC_OK;
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *err = std::string("CUDA error: ") + cudaGetErrorString(e) + " (scan table allocation)";
+    rc = GSMC_E_CUDA;
+  } else if (build_tables_gpu_f64(ff, L, 4.0 * ne * rho, 4.0 * ne * mu, ts->site, ts->chunk,
+                                  &ts->hom_m, &ts->hom_c, err) != 0) {
+    rc = GSMC_E_CUDA;
+  }
+  cudaSetDevice(prev);
+  return rc;
+}
+
+// Build and upload of one set (no lock held): the host float32 build that
+// matches the reference bit for bit, or the float64 GPU build.
+int build_table_set(const char* ff_path, double ne_d, double mu_d, double rho_d, int L, bool f64,
+                    TableSet* ts, std::string* err) {
+  FlowField ff;
+  char buf[512];
+  if (load_flow_field(ff_path, &ff, buf, sizeof(buf)) != 0) {
+    *err = buf;
+    return GSMC_E_IO;
+  }
+  if (f64) return build_table_set_f64(ff, ne_d, mu_d, rho_d, L, ts, err);
+  const float ne = (float)ne_d, mu = (float)mu_d, rho = (float)rho_d;
+  float srho, smu;
+  scaled_rates(ne, mu, rho, &srho, &smu);
+  HostLayers layers;
+  build_layers(ff, L, srho, smu, 0, &layers);
+  std::vector<float> site, chunk;
+  build_scan_layout(layers, &site, &chunk, 0);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaError_t e = cudaSetDevice(ts->device);
+  if (e == cudaSuccess) e = cudaMalloc(&ts->site, site.size() * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&ts->chunk, chunk.size() * sizeof(float));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(ts->site, site.data(), site.size() * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(ts->chunk, chunk.data(), chunk.size() * sizeof(float), cudaMemcpyHostToDevice);
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *err = std::string("CUDA error: ") + cudaGetErrorString(e) + " (scan table upload)";
+    return GSMC_E_CUDA;
+  }
+  ts->hom_m = std::move(layers.t[kHomMean]);
+  ts->hom_c = std::move(layers.t[kHomCv]);
+  return GSMC_OK;
+}
+
+// The set for a key, built if needed; *reused is false when this call built
+// it.
+int acquire_tables(int device, const char* ff_path, double ne, double mu, double rho, int L,
+                   bool f64, TableSet** out, bool* reused) {
+  const TableKey key{device, std::string(ff_path), (float)ne, (float)mu, (float)rho, L, f64};
+  std::unique_lock<std::mutex> lock(g_tables_mu);
+  auto it = g_tables.find(key);
+  if (it != g_tables.end()) {
+    TableSet* ts = it->second;
+    if (ts->refs++ == 0) {
+      auto pk = g_parked.find(device);
+      if (pk != g_parked.end() && pk->second == ts) g_parked.erase(pk);
+    }
+    g_tables_cv.wait(lock, [ts] { return ts->ready; });
+    if (ts->status != GSMC_OK) {
+      const int st = ts->status;
+      const std::string msg = ts->error;
+      drop_ref_locked(ts);
+      return fail(st, "%s", msg.c_str());
+    }
+    *out = ts;
+    *reused = true;
+    return GSMC_OK;
+  }
+  TableSet* ts = new TableSet;
+  ts->device = device;
+  ts->L = L;
+  ts->refs = 1;
+  g_tables[key] = ts;
+  lock.unlock();
+  const auto t0 = std::chrono::steady_clock::now();
+  std::string err;
+  const int st = build_table_set(ff_path, ne, mu, rho, L, f64, ts, &err);
+  const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  lock.lock();
+  ts->build_seconds = secs;
+  ts->status = st;
+  ts->error = err;
+  ts->ready = true;
+  g_tables_cv.notify_all();
+  if (st != GSMC_OK) {
+    erase_key_of(ts);
+    drop_ref_locked(ts);
+    return fail(st, "%s", err.c_str());
+  }
+  *out = ts;
+  *reused = false;
+  return GSMC_OK;
+}
+
+void release_tables(TableSet* ts) {
+  if (!ts) return;
+  std::lock_guard<std::mutex> lock(g_tables_mu);
+  drop_ref_locked(ts);
 }
 
 // max(1, round-half-even(delta)) (src/kernels/gamma_smc_flow.cu:160-163).
@@ -175,6 +286,8 @@ struct gsmc_ctx {
   ulonglong2* geno = nullptr;
   SiteCode* code = nullptr;  // site 0 of the code array (kCodePad entries before it)
   TableSet* tables = nullptr;
+  double tables_build_seconds = 0.0;  // this context's table build and upload
+  bool tables_reused = false;         // the tables were resident already
   ScanShape shape{128, 1};  // scan launch shape of the current call (pick_shape)
   bool shape_fixed = false; // shape set by the environment, not per call
   cudaStream_t stream = nullptr;
@@ -197,6 +310,7 @@ struct gsmc_ctx {
   void* repair_pool = nullptr;            // forward-state slots of the repair launch
   size_t repair_pool_bytes = 0;
   bool speculate = true;                  // GSMC_SPECULATE=0 turns chunking off
+  int spec_chunks_fixed = 0;              // GSMC_SPEC_CHUNKS: chunks per window, for measurements
   int64_t spec_flank = 2048;              // burn-in sites of a speculative chunk
   int64_t spec_launches = 0;              // launches that ran speculative chunks
   int* spec_repaired = nullptr;           // device: (window, pair)s repaired so far
@@ -453,6 +567,8 @@ struct SpecLaunch {
 int spec_chunks(const gsmc_ctx* ctx, int64_t tasks, int64_t resident_tiles, int64_t core_len,
                 int flags) {
   if (!ctx->speculate || (flags & kTaskSummary) || tasks <= 0) return 1;
+  if (ctx->spec_chunks_fixed > 0)
+    return (int)std::max<int64_t>(1, std::min<int64_t>(ctx->spec_chunks_fixed, core_len / 64));
   if (tasks >= 2 * resident_tiles) return 1;
   const int64_t want = ceil_div(2 * resident_tiles, tasks);
   return (int)std::max<int64_t>(1, std::min<int64_t>(want, core_len / (4 * ctx->spec_flank)));
@@ -770,6 +886,13 @@ int gsmc_get_device(int* device) {
 int gsmc_ctx_create(const uint8_t* G, int64_t n_haps, int64_t n_sites, const double* positions,
                     double Ne, double mu, double rho, const char* flow_field_path,
                     int cache_steps, gsmc_ctx** out) {
+  return gsmc_ctx_create_ex(G, n_haps, n_sites, positions, Ne, mu, rho, flow_field_path,
+                            cache_steps, 0, out);
+}
+
+int gsmc_ctx_create_ex(const uint8_t* G, int64_t n_haps, int64_t n_sites, const double* positions,
+                       double Ne, double mu, double rho, const char* flow_field_path,
+                       int cache_steps, int flags, gsmc_ctx** out) {
   if (!out) return fail(GSMC_E_INVALID, "null output handle");
   *out = nullptr;
   if (n_haps < 0 || n_sites < 0) return fail(GSMC_E_INVALID, "negative genotype shape");
@@ -794,13 +917,20 @@ int gsmc_ctx_create(const uint8_t* G, int64_t n_haps, int64_t n_sites, const dou
   if (const char* env = std::getenv("GSMC_SPECULATE")) ctx->speculate = std::atoi(env) != 0;
   if (const char* env = std::getenv("GSMC_SPEC_FLANK"))
     ctx->spec_flank = std::max<int64_t>(1, std::atoll(env));
+  if (const char* env = std::getenv("GSMC_SPEC_CHUNKS"))
+    ctx->spec_chunks_fixed = std::max(0, std::atoi(env));
   if (const char* env = std::getenv("GSMC_SCAN_WIDTH")) {
     const int v = std::atoi(env);
     if (v == 32 || v == 128) ctx->shape.width = v;
     ctx->shape_fixed = true;
   }
-  int rc = acquire_tables(ctx->device, flow_field_path, (float)Ne, (float)mu, (float)rho, L,
-                          &ctx->tables);
+  bool reused = false;
+  int rc = acquire_tables(ctx->device, flow_field_path, Ne, mu, rho, L,
+                          (flags & GSMC_TABLES_GPU_F64) != 0, &ctx->tables, &reused);
+  if (rc == GSMC_OK) {
+    ctx->tables_reused = reused;
+    ctx->tables_build_seconds = reused ? 0.0 : ctx->tables->build_seconds;
+  }
   if (rc) return rc;
   struct Guard {
     std::unique_ptr<gsmc_ctx>* p;
@@ -1704,6 +1834,23 @@ int gsmc_flow_fb(const uint8_t* G, int64_t n_haps, int64_t n_sites, const double
   return GSMC_OK;
 }
 
+int gsmc_ctx_tables_info(const gsmc_ctx* ctx, double* build_seconds, int* reused) {
+  if (int rc = check_ctx(ctx)) return rc;
+  if (build_seconds) *build_seconds = ctx->tables_build_seconds;
+  if (reused) *reused = ctx->tables_reused ? 1 : 0;
+  return GSMC_OK;
+}
+
+int gsmc_free_cached_tables(void) {
+  std::lock_guard<std::mutex> lock(g_tables_mu);
+  for (auto& kv : g_parked) {
+    erase_key_of(kv.second);
+    free_table_set(kv.second);
+  }
+  g_parked.clear();
+  return GSMC_OK;
+}
+
 int gsmc_set_copy_wait_polls(int64_t polls, int64_t* previous) {
   if (polls < 0) return fail(GSMC_E_INVALID, "the poll budget must be non-negative");
   const long long prev = g_copy_wait_polls.exchange(polls);
@@ -1792,8 +1939,8 @@ int gsmc_ctx_table_layer(const gsmc_ctx* ctx, int table, int layer, float* out) 
       const int pr = std::min(r, kPatchRows - 1), pq = std::min(q, kPatchCols - 1);
       const int corner = (r - pr) * 2 + (q - pq);
       const float* p = patches.data() + (size_t)(pr * kPatchCols + pq) * 8;
-      out[r * kCols + q] = p[corner];
-      out[kCells + r * kCols + q] = p[4 + corner];
+      out[r * kCols + q] = p[2 * corner];
+      out[kCells + r * kCols + q] = p[2 * corner + 1];
     }
   return GSMC_OK;
 }

@@ -101,6 +101,36 @@ const std::vector<float>& cv_cap() {
   return cap;
 }
 
+}  // namespace
+
+// The same cap kept in float64 (the bisection's final upper bound), for the
+// float64 table build.
+const std::vector<double>& cv_cap_f64() {
+  static const std::vector<double> cap = [] {
+    const int n = (int)std::llround(kCapMeanHi / kCapMeanStep) + 1;
+    std::vector<double> out(n);
+    for (int i = 0; i < n; ++i) {
+      const double ml = i * kCapMeanStep;
+      double lo = -2.0, hi = 0.0;
+      if (entropy(ml, lo) > 1.0) {
+        out[i] = lo;
+      } else if (entropy(ml, hi) <= 1.0) {
+        out[i] = hi;
+      } else {
+        for (int it = 0; it < 60; ++it) {
+          const double mid = 0.5 * (lo + hi);
+          (entropy(ml, mid) > 1.0 ? hi : lo) = mid;
+        }
+        out[i] = hi;
+      }
+    }
+    return out;
+  }();
+  return cap;
+}
+
+namespace {
+
 // Grid clamp plus the entropy cap (src/flow_field.cpp:150-166).
 inline void clip(float& m, float& c, const GridSpec& g, const std::vector<float>& cap) {
   m = std::max(g.m_lo, std::min(m, g.m_hi));
@@ -269,23 +299,38 @@ void scaled_rates(double Ne, double mu, double rho, float* scaled_rho, float* sc
   *scaled_mu = 4.0f * ne * (float)mu;
 }
 
-// Scan layout: one 32-byte patch per interpolation cell (r, q), r < 50,
+// Planar patch: one 8-value patch per interpolation cell (r, q), r < 50,
 // q < 49, holding the four corners of m then of c:
 //   {m[r][q], m[r][q+1], m[r+1][q], m[r+1][q+1]}, {c[r][q], ..., c[r+1][q+1]}
-// so one lookup is two 16-byte loads from a single 32-byte sector.
+// (the forward-only path's half-precision table converts this layout).
 void pack_patches(const float* m, const float* c, float* dst) {
   for (int r = 0; r < kPatchRows; ++r)
     for (int q = 0; q < kPatchCols; ++q) {
       const int a = r * kCols + q;
+      const int corner[4] = {a, a + 1, a + kCols, a + kCols + 1};
       float* p = dst + (size_t)(r * kPatchCols + q) * 8;
-      p[0] = m[a];
-      p[1] = m[a + 1];
-      p[2] = m[a + kCols];
-      p[3] = m[a + kCols + 1];
-      p[4] = c[a];
-      p[5] = c[a + 1];
-      p[6] = c[a + kCols];
-      p[7] = c[a + kCols + 1];
+      for (int k = 0; k < 4; ++k) {
+        p[k] = m[corner[k]];
+        p[4 + k] = c[corner[k]];
+      }
+    }
+}
+
+// Scan layout: one 32-byte patch per interpolation cell (r, q), r < 50,
+// q < 49, holding the (m, c) pair of each corner:
+//   {m, c}[r][q], {m, c}[r][q+1], {m, c}[r+1][q], {m, c}[r+1][q+1]
+// so one lookup is a single 256-bit load whose four 64-bit quarters are the
+// packed (m, c) operands of the scan's two-lane interpolation.
+void pack_patches_mc(const float* m, const float* c, float* dst) {
+  for (int r = 0; r < kPatchRows; ++r)
+    for (int q = 0; q < kPatchCols; ++q) {
+      const int a = r * kCols + q;
+      const int corner[4] = {a, a + 1, a + kCols, a + kCols + 1};
+      float* p = dst + (size_t)(r * kPatchCols + q) * 8;
+      for (int k = 0; k < 4; ++k) {
+        p[2 * k] = m[corner[k]];
+        p[2 * k + 1] = c[corner[k]];
+      }
     }
 }
 
@@ -302,14 +347,14 @@ void build_scan_layout(const HostLayers& h, std::vector<float>* site, std::vecto
   parallel_for((long long)kScanTables * L, threads, [&](long long lo, long long hi) {
     for (long long tl = lo; tl < hi; ++tl) {
       const int t = (int)(tl / L), k = (int)(tl % L);
-      pack_patches(h.t[kSrc[t][0]].data() + (size_t)k * kCells,
-                   h.t[kSrc[t][1]].data() + (size_t)k * kCells,
-                   site->data() + scan_layer_offset(t, k, L) * 4);
+      pack_patches_mc(h.t[kSrc[t][0]].data() + (size_t)k * kCells,
+                      h.t[kSrc[t][1]].data() + (size_t)k * kCells,
+                      site->data() + scan_layer_offset(t, k, L) * 4);
     }
   });
   chunk->assign(per_layer, 0.0f);
-  pack_patches(h.t[kHomMean].data() + (size_t)(L - 1) * kCells,
-               h.t[kHomCv].data() + (size_t)(L - 1) * kCells, chunk->data());
+  pack_patches_mc(h.t[kHomMean].data() + (size_t)(L - 1) * kCells,
+                  h.t[kHomCv].data() + (size_t)(L - 1) * kCells, chunk->data());
 }
 
 }  // namespace gsmc

@@ -36,7 +36,8 @@ struct HostLayers {
 };
 
 // Scan tables on the device: [direction][n_steps][hom, het][kPatches][8]
-// floats, so the hom and het patches of one layer are adjacent and a pair's
+// floats (patches of pack_patches_mc), so the hom and het patches of one
+// layer are adjacent and a pair's
 // het bit selects between them with one multiply-add.  Offsets below are in
 // float4 units (two per patch).
 enum ScanTable { kScanFwdHom = 0, kScanFwdHet, kScanBwdHom, kScanBwdHet, kScanTables };
@@ -51,11 +52,18 @@ inline size_t scan_layer_offset(int table, int layer, int L) {
   return ((size_t)dir * L + layer) * kLayerF4 + (size_t)het * kHetF4;
 }
 
+// The entropy cap on log10 CV at log10 mean 0, 0.0008, ..., 4 in float64
+// (the float64 table build's copy of the builder's float table).
+const std::vector<double>& cv_cap_f64();
+
 int load_flow_field(const char* path, FlowField* ff, char* err, size_t err_len);
 void scaled_rates(double Ne, double mu, double rho, float* scaled_rho, float* scaled_mu);
 void build_layers(const FlowField& ff, int n_steps, float scaled_rho, float scaled_mu,
                   int threads, HostLayers* out);
+// 2450 patches of 8 floats from one [51 x 50] (m, c) layer: planar (m
+// corners, then c corners) or interleaved ((m, c) per corner, the scan's).
 void pack_patches(const float* m, const float* c, float* dst);
+void pack_patches_mc(const float* m, const float* c, float* dst);
 void build_scan_layout(const HostLayers& h, std::vector<float>* site,
                        std::vector<float>* chunk, int threads);
 

@@ -76,6 +76,27 @@ int gsmc_ctx_create(const uint8_t* G, int64_t n_haps, int64_t n_sites,
                     const char* flow_field_path, int cache_steps,
                     gsmc_ctx** out);
 
+/* Flags of gsmc_ctx_create_ex. */
+enum {
+  /* Build the scan tables on the GPU in float64 (every cell's chain carried
+   * in float64, rounded to float32 only when stored) instead of the host
+   * float32 build that reproduces the reference's tables bit for bit. */
+  GSMC_TABLES_GPU_F64 = 1
+};
+
+/*
+ * gsmc_ctx_create with flags (GSMC_TABLES_GPU_F64).  The float64 tables are a
+ * separate resident set from the float32 ones of the same parameters; results
+ * through them differ from the reference's in the last bits of the tables
+ * (the deviation of the posterior means is measured by the tests and the
+ * benchmark).  Replaces the same reference code as gsmc_ctx_create, plus the
+ * table build the reference does on the host (src/flow_field.cpp:205-388).
+ */
+int gsmc_ctx_create_ex(const uint8_t* G, int64_t n_haps, int64_t n_sites,
+                       const double* positions, double Ne, double mu, double rho,
+                       const char* flow_field_path, int cache_steps, int flags,
+                       gsmc_ctx** out);
+
 /* Release a context (FlowContext::~FlowContext, src/bindings.cpp:2672-2677). */
 int gsmc_ctx_destroy(gsmc_ctx* ctx);
 
@@ -403,6 +424,23 @@ int gsmc_flow_fb(const uint8_t* G, int64_t n_haps, int64_t n_sites, const double
                  const int32_t* pair_i, const int32_t* pair_j, int64_t n_pairs, double Ne,
                  double mu, double rho, const char* flow_field_path, int flags, float* mean,
                  float* lower, float* upper);
+
+/*
+ * Table build of a context: *build_seconds = build + upload of its scan
+ * tables by this context (0 when it reused a resident set), *reused = 1 when
+ * a set with the same (device, flow field, Ne, mu, rho, cache_steps, build)
+ * was resident already (held by another context, or parked: the most
+ * recently released set of each device stays resident, as the reference's
+ * process-wide table cache does, src/bindings.cpp:1884-2157).  Either
+ * pointer may be NULL.
+ */
+int gsmc_ctx_tables_info(const gsmc_ctx* ctx, double* build_seconds, int* reused);
+
+/*
+ * Free the parked table sets (those no live context holds); sets in use stay.
+ * No reference counterpart.
+ */
+int gsmc_free_cached_tables(void);
 
 /*
  * Poll budget of the uncached kernels' wait for their shared-memory copy of

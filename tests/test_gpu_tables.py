@@ -76,7 +76,7 @@ def test_concurrent_creation_and_parked_reuse(data, flow_field):
     for c in ctxs:
         c.close()
     # the last set released stays resident for the next context with it
-    last = [c for c in range(6)][-1] % 3
+    last = 5 % 3   # contexts closed in order: the last one released holds PARAMS[2]
     again = _core.FlowContext(G, pos, *PARAMS[last], flow_field, 0)
     assert again.tables_info() == {"build_seconds": 0.0, "reused": True}
     _same(again.run_fb(pairs, mean_only=False, return_posterior=True), want[last])

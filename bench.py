@@ -554,8 +554,8 @@ def run_reference_gpu(G, pos, pairs, core, flank, mu, rho, cols, ours_cols, e2e,
     S, P = G.shape[1], len(pairs)
     sites = S
     avail = psutil.virtual_memory().available
-    if 4.0 * S * P > 0.6 * avail:
-        sites = int(0.6 * avail / (4.0 * P))
+    if 4.0 * S * P > 0.45 * avail:
+        sites = int(0.45 * avail / (4.0 * P))
     Gs, ps = np.ascontiguousarray(G[:, :sites]), np.ascontiguousarray(pos[:sites])
     plist = [tuple(p) for p in pairs.tolist()]
     t0 = time.perf_counter()
@@ -572,6 +572,8 @@ def run_reference_gpu(G, pos, pairs, core, flank, mu, rho, cols, ours_cols, e2e,
     if e2e is not None and e2e.get("sites") == sites:
         job["ours_e2e_seconds"] = e2e["seconds_per_step"]
         job["speedup_e2e"] = t / e2e["seconds_per_step"]
+        job["ours_e2e_pageable_seconds"] = e2e["pageable_seconds"]
+        job["speedup_e2e_pageable"] = t / e2e["pageable_seconds"]
     # the reference's kernels alone, on 8,192 of the pairs (CUPTI activity
     # records of one run, taken separately from the wall-clock run above)
     sub = plist[:kernel_pairs]
@@ -684,11 +686,39 @@ def run_batched(ctx, G, dev, plain_jobs, jobs=None, workload=BATCH_WORKLOAD):
         got = bs.to_host()
         batched_s = time.perf_counter() - t0
         del bs
+    # the same batch with its results landing by DMA in a pinned buffer that
+    # is reused batch after batch (the server's result arena): the results are
+    # views into it, so no host thread copies or page-faults them
+    from gamma_smc_cu_b200.serve import PinnedArena
+    arena = PinnedArena(Layout(sample).out_floats * 4 + (1 << 20))
+    for rep in range(3):
+        t0 = time.perf_counter()
+        bs = DeviceBatch(Layout(sample), dev)
+        bs.launch(ex, st, host=arena.alloc(bs.layout.out_floats * 4))
+        got_pinned = bs.results()
+        pinned_s = time.perf_counter() - t0
+        err_pinned = max(_max_rel(g["mean"], w["mean"]) for g, w in zip(got_pinned, got))
+        del bs, got_pinned
     big = max(sample, key=lambda j: j.pair_sites)   # grow the per-call scratch first
     ctx.run_fb_window(big.pairs, big.site_begin, big.site_end)
     t0 = time.perf_counter()
     want = [ctx.run_fb_window(j.pairs, j.site_begin, j.site_end) for j in sample]
     plain_s = time.perf_counter() - t0
+    # the plain per-call path with page-locked result buffers too (second pass:
+    # the first one fills the buffer cache)
+    from gamma_smc_cu_b200 import _core, _lib
+    prev = _core.set_result_memory("pinned")
+    try:
+        for rep in range(2):
+            t0 = time.perf_counter()
+            for j in sample:
+                r = ctx.run_fb_window(j.pairs, j.site_begin, j.site_end)
+                del r
+            plain_pinned_s = time.perf_counter() - t0
+    finally:
+        _core.set_result_memory(prev)
+        _lib.check(_lib.load().gsmc_host_cache_limit(0))        # give the memory back
+        _lib.check(_lib.load().gsmc_host_cache_limit(256 << 30))
     err = max(_max_rel(g["mean"], w["mean"]) for g, w in zip(got, want))
     ex.close()
     return {"workload": workload, "pair_sites": total, "device_ms": dev_ms, "kernel_ms": kms / max(1, reps),
@@ -698,9 +728,13 @@ def run_batched(ctx, G, dev, plain_jobs, jobs=None, workload=BATCH_WORKLOAD):
             "tune_seconds": tune_s, "tune_trials": tuned["searched"],
             "sample_jobs": len(sample), "sample_pair_sites": sample_ps,
             "sample_batched_e2e": sample_ps / batched_s,
+            "sample_batched_pinned_e2e": sample_ps / pinned_s,
             "sample_plain_per_call": sample_ps / plain_s,
-            "speedup_vs_plain": plain_s / batched_s,
-            "max_rel_mean_vs_plain": err}
+            "sample_plain_per_call_pinned": sample_ps / plain_pinned_s,
+            "speedup_vs_plain": plain_s / pinned_s,
+            "speedup_vs_plain_numpy_out": plain_s / batched_s,
+            "speedup_vs_plain_pinned": plain_pinned_s / pinned_s,
+            "max_rel_mean_vs_plain": max(err, err_pinned)}
 
 
 def run_summary(ctx, pairs, S, steps=2):
@@ -833,6 +867,12 @@ def run_served(dev, rates=(10, 100, 1000, 2000), seconds=2.0, burst=300):
                 "served_service_p99_ms": st["service_p99_ms"],
                 "served_pair_sites_per_s": st["pair_sites_per_s"],
                 "served_batches": st.get("batches"),
+                "served_max_ms": st.get("max_ms"),
+                "served_gc_pauses": st.get("gc_pauses"), "served_gc_max_ms": st.get("gc_max_ms"),
+                "served_loop_stalls_ms": st.get("loop_stalls_ms"),
+                "served_waits": {k: st.get(k, 0) for k in ("wait_executor", "wait_hbm",
+                                                            "wait_arena", "outside_arena",
+                                                            "redone_whole")},
                 "plain_p50_ms": float(np.percentile(lat, 50) * 1e3),
                 "plain_p99_ms": float(np.percentile(lat, 99) * 1e3),
                 "plain_pair_sites_per_s": ps / wall}
@@ -898,39 +938,65 @@ def run_stream_stress(core=8192, flank=2048):
 
 
 def run_e2e(G, pos, pairs, core, flank, steps):
-    """Public API with host buffers: context (H2D genotypes), blockwise run,
-    D2H of every posterior into numpy."""
+    """Public API with host buffers: context (H2D genotypes and positions),
+    blockwise run, D2H of every posterior into host arrays.  Timed with the
+    results in page-locked buffers that the DMA writes directly
+    (set_result_memory("pinned"); the buffers and the scan tables are made by
+    an untimed first call and reused by the timed ones, as a repeated caller
+    sees them), and once more into fresh pageable numpy arrays."""
     import psutil
-    from gamma_smc_cu_b200 import _core
+    from gamma_smc_cu_b200 import _core, _lib
     from gamma_smc_cu_b200.infer import _estimate_scaled_params
     S, P = G.shape[1], len(pairs)
     avail = psutil.virtual_memory().available
     sites = S
-    if 4.0 * S * P > 0.6 * avail:
-        sites = int(0.6 * avail / (4.0 * P))
+    if 4.0 * S * P > 0.45 * avail:
+        sites = int(0.45 * avail / (4.0 * P))
     Gs, ps = np.ascontiguousarray(G[:, :sites]), np.ascontiguousarray(pos[:sites])
     mu, rho = _estimate_scaled_params(Gs, ps, 1.25e-8, 1e-8, 1e4)
     plist = [tuple(p) for p in pairs.tolist()]
 
     def once():
+        t0 = time.perf_counter()
         ctx = _core.FlowContext(Gs, ps, 1e4, mu, rho, _core.DEFAULT_FLOW_FIELD, 0)
+        t_ctx = time.perf_counter() - t0
+        info = ctx.tables_info()
         r = ctx.run_fb_blockwise(plist, core_block_sites=core, flank_sites=flank,
                                  pair_batch_size=P, max_streams=1, mean_only=True)
         ctx.close()
-        return r
+        return r, info, t_ctx
 
-    r = once()  # warm-up (tables built once per parameter set, as in the reference)
-    del r
-    times = []
-    for _ in range(max(1, steps)):
+    prev = _core.set_result_memory("pinned")
+    try:
         t0 = time.perf_counter()
-        r = once()
-        times.append(time.perf_counter() - t0)
+        r, info0, _ = once()   # builds the tables and the page-locked result buffer
+        first_s = time.perf_counter() - t0
         del r
+        times, ctx_s = [], []
+        for _ in range(max(1, steps)):
+            t0 = time.perf_counter()
+            r, info, t_ctx = once()
+            times.append(time.perf_counter() - t0)
+            ctx_s.append(t_ctx)
+            del r
+    finally:
+        _core.set_result_memory(prev)
+        _lib.check(_lib.load().gsmc_host_cache_limit(0))        # give the memory back
+        _lib.check(_lib.load().gsmc_host_cache_limit(256 << 30))
+    t0 = time.perf_counter()
+    r, _, _ = once()
+    pageable_s = time.perf_counter() - t0
+    del r
     t = float(np.mean(times))
-    return {"value": P * sites / t, "unit": UNIT, "h2d_bytes_per_step": int(Gs.nbytes + ps.nbytes + 8 * P),
+    return {"value": P * sites / t, "unit": UNIT,
+            "h2d_bytes_per_step": int(Gs.nbytes + ps.nbytes + 8 * P),
             "d2h_bytes_per_step": int(4 * sites * P), "seconds_per_step": t, "sites": sites,
-            "steps": len(times)}
+            "steps": len(times), "result_memory": "page-locked buffers reused across calls",
+            "context_seconds_per_step": float(np.mean(ctx_s)),
+            "first_call_seconds": first_s,
+            "table_build_seconds_first_call": info0["build_seconds"],
+            "tables_reused_in_timed_steps": bool(info["reused"]),
+            "pageable_seconds": pageable_s, "pageable_value": P * sites / pageable_s}
 
 
 # ------------------------------------------------------------ profiling cases
@@ -943,6 +1009,9 @@ def run_e2e(G, pos, pairs, core, flank, steps):
 #             pairs: the two-pairs-per-thread shape of the full job), mean-only
 #   full      cached FB, mean + alpha + beta, 4,096 sites x 63,190 pairs,
 #             blockwise core 256 / flank 64 (16 windows, two pairs per thread)
+#   full_slice  cached FB, mean + alpha + beta, one 50,000-site window x 8,192
+#             pairs in exact speculative chunks (the full-posterior slice's
+#             shape), two pairs per thread
 #   batch     64 uneven jobs (1-2,000 pairs, 2k-40k-site windows) over a
 #             60,000-site slice, one executor launch (32-thread tiles,
 #             4,096-site chunks)
@@ -997,6 +1066,29 @@ def case_full(repeat):
             None))
     torch.cuda.synchronize()
     print("scan shape", ctx.scan_shape())
+
+
+def case_full_slice(repeat):
+    """The full-posterior slice's shape at 8,192 pairs: one 50,000-site window
+    (core = the whole slice, flank 2,048), mean + alpha + beta, exact
+    speculative chunks with 2,048-site burn-ins, two pairs per thread."""
+    import torch
+    from gamma_smc_cu_b200 import _lib, synthetic
+    os.environ["GSMC_PAIRS_PER_THREAD"] = "2"
+    ctx, G, pos = _case_ctx(50000)
+    pairs = synthetic.random_pairs(G.shape[0], 8192, 31)
+    dev = torch.device("cuda", ctx.device_id)
+    pi = torch.from_numpy(np.ascontiguousarray(pairs[:, 0])).to(dev)
+    pj = torch.from_numpy(np.ascontiguousarray(pairs[:, 1])).to(dev)
+    S, P = G.shape[1], len(pairs)
+    outs = [torch.empty((S, P), device=dev) for _ in range(3)]
+    L = _lib.load()
+    for _ in range(1 + repeat):
+        _lib.check(L.gsmc_run_fb_blockwise_device(
+            ctx.handle, pi.data_ptr(), pj.data_ptr(), P, S, 2048, _lib.GSMC_POSTERIOR,
+            outs[0].data_ptr(), None, None, outs[1].data_ptr(), outs[2].data_ptr(), P, 0, None))
+    torch.cuda.synchronize()
+    print("scan shape", ctx.scan_shape(), "speculative", ctx.spec_stats())
 
 
 def case_batch(repeat):
@@ -1066,12 +1158,8 @@ def case_uncached_spec(repeat):
         _core.gamma_smc_flow_fb(G, pos, pairs, mean_only=True)
 
 
-CASES = {"scan": case_scan, "full": case_full, "batch": case_batch, "summary": case_summary, "fwd": case_fwd,
-         "uncached": case_uncached, "flowgen": case_flowgen, "fwd_spec": case_fwd_spec,
-         "uncached_spec": case_uncached_spec}
-
-
-CASES = {"scan": case_scan, "full": case_full, "batch": case_batch, "summary": case_summary,
+CASES = {"scan": case_scan, "full": case_full, "full_slice": case_full_slice, "batch": case_batch,
+         "summary": case_summary,
          "fwd": case_fwd, "uncached": case_uncached, "flowgen": case_flowgen,
          "fwd_spec": case_fwd_spec, "uncached_spec": case_uncached_spec}
 

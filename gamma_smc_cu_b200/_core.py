@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import weakref
 
 import numpy as np
 
@@ -104,6 +105,51 @@ def gamma_smc_flow_fb(G, positions, pairs, Ne=10000.0, mu=1.25e-8, rho=1e-8,
     return out
 
 
+_RESULT_MEMORY = os.environ.get("GSMC_RESULT_MEMORY", "pageable")
+
+
+def set_result_memory(kind):
+    """Where the host result arrays of this module's calls live (no reference
+    counterpart).  "pageable" (default): fresh numpy arrays, filled through
+    the library's pinned staging ring by host threads.  "pinned": arrays in
+    page-locked buffers that the device-to-host DMA writes directly; a buffer
+    returns to a cache when its last array is dropped and is reused by later
+    calls it fits, so repeated large calls skip both the staging copy and the
+    first-touch page faults.  Allocating page-locked memory the first time is
+    slow (seconds per 100 GB), so "pinned" pays off from the second call of a
+    size on.  Returns the previous setting."""
+    global _RESULT_MEMORY
+    if kind not in ("pageable", "pinned"):
+        raise ValueError("result memory must be 'pageable' or 'pinned'")
+    prev, _RESULT_MEMORY = _RESULT_MEMORY, kind
+    return prev
+
+
+def _free_host(ptr):
+    if _lib._lib is not None:
+        _lib._lib.gsmc_host_free(ctypes.c_void_p(ptr))
+
+
+class _HostBlock:
+    """A page-locked buffer from the library's cache; numpy views keep it
+    alive and it returns to the cache when the last one goes."""
+
+    def __init__(self, nbytes):
+        p = ctypes.c_void_p()
+        check(_lib.load().gsmc_host_alloc(int(nbytes), ctypes.byref(p)))
+        self.__array_interface__ = {"shape": (int(nbytes) // 4,), "typestr": "<f4",
+                                    "data": (p.value, False), "version": 3}
+        weakref.finalize(self, _free_host, p.value)
+
+
+def _empty(shape):
+    """float32 result array of ``shape`` in the memory set_result_memory chose."""
+    n = int(np.prod(shape))
+    if _RESULT_MEMORY == "pinned" and n > 0:
+        return np.asarray(_HostBlock(4 * n))[:n].reshape(shape)
+    return np.empty(shape, np.float32)
+
+
 def free_cached_tables():
     """Free the scan-table sets no live context holds (the most recently
     released set of each device otherwise stays resident for the next context
@@ -188,13 +234,13 @@ class FlowContext:
         return self._S
 
     def _outputs(self, rows, P, ci, posterior):
-        out = {"mean": np.empty((rows, P), np.float32)}
+        out = {"mean": _empty((rows, P))}
         if ci:
-            out["lower"] = np.empty((rows, P), np.float32)
-            out["upper"] = np.empty((rows, P), np.float32)
+            out["lower"] = _empty((rows, P))
+            out["upper"] = _empty((rows, P))
         if posterior:
-            out["posterior_alpha"] = np.empty((rows, P), np.float32)
-            out["posterior_beta"] = np.empty((rows, P), np.float32)
+            out["posterior_alpha"] = _empty((rows, P))
+            out["posterior_beta"] = _empty((rows, P))
         return out
 
     @staticmethod

@@ -133,6 +133,9 @@ SIGNATURES = {
     "gsmc_set_copy_wait_polls": (c_int, [c_i64, c_i64p]),
     "gsmc_ctx_tables_info": (c_int, [c_vp, ctypes.POINTER(ctypes.c_double), c_intp]),
     "gsmc_free_cached_tables": (c_int, []),
+    "gsmc_host_alloc": (c_int, [ctypes.c_uint64, ctypes.POINTER(c_vp)]),
+    "gsmc_host_free": (c_int, [c_vp]),
+    "gsmc_host_cache_limit": (c_int, [ctypes.c_uint64]),
     "gsmc_bitpack": (c_int, [c_u8p, c_i64, c_i64, c_u64p]),
     "gsmc_unpack": (c_int, [c_u64p, c_i64, c_i64, c_u8p]),
     "gsmc_ctx_table_layer": (c_int, [c_vp, c_int, c_int, c_f32p]),

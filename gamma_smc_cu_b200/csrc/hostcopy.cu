@@ -132,7 +132,14 @@ int HostCopier::enqueue(void* dst, size_t dpitch, const void* src, size_t spitch
   if (rows == 0 || width == 0) return cudaSuccess;
   cudaError_t e = cudaStreamWaitEvent(m.stream, ready, 0);
   if (e != cudaSuccess) return e;
-  if (width > kSlotBytes) {  // cannot stage: plain pageable copy on the stream
+  // A page-locked destination (cudaHostAlloc, cudaHostRegister, the result
+  // buffers of gsmc_host_alloc) takes the DMA directly: no staging, no host
+  // thread touches the data.
+  cudaPointerAttributes attr;
+  const bool pinned = cudaPointerGetAttributes(&attr, dst) == cudaSuccess &&
+                      attr.type == cudaMemoryTypeHost;
+  if (!pinned) cudaGetLastError();  // pageable memory may report an error on older drivers
+  if (pinned || width > kSlotBytes) {  // direct: page-locked, or too wide to stage
     {
       std::lock_guard<std::mutex> l(m.mu);
       m.direct = true;

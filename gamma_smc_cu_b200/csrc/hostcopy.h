@@ -5,7 +5,9 @@
 // copier instead moves rows through a ring of pinned buffers on its own copy
 // stream, and a pool of host threads moves each landed buffer into the
 // destination in parallel (taking the destination's first-touch page faults
-// in parallel too), overlapping both with the GPU's compute.
+// in parallel too), overlapping both with the GPU's compute.  A destination
+// that is page-locked already (gsmc_host_alloc's result buffers, or any
+// cudaHostAlloc'd / registered memory) is written by the DMA directly.
 #pragma once
 
 #include <cuda_runtime.h>

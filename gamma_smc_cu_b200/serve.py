@@ -24,6 +24,7 @@ admission counters.
 from __future__ import annotations
 
 import collections
+import gc
 import threading
 import time
 import weakref
@@ -161,7 +162,8 @@ class TmrcaServer:
     def __init__(self, ctx, positions=None, max_inflight=3, core_block_sites=4096,
                  flank_sites=2048, tile_width=128, pairs_per_thread=1, use_graph=True,
                  hbm_budget=None, max_tasks=1 << 15, max_batch_requests=4096,
-                 max_batch_pair_sites=1 << 29, pinned_bytes=1 << 30, poll_interval=50e-6):
+                 max_batch_pair_sites=1 << 29, pinned_bytes=1 << 30, poll_interval=50e-6,
+                 freeze_gc=True):
         self.ctx = ctx
         self.positions = None if positions is None else np.asarray(positions, np.float64)
         self.device = ctx.device_id
@@ -191,6 +193,22 @@ class TmrcaServer:
         self._redo_ex = None
         self._redo_tasks = 0
         self._redo_stream = None
+        # Diagnostics of the latency tail: the longest scheduler-loop stalls
+        # (what the loop was doing), and the cyclic garbage collector's pauses
+        # while serving (they stop the scheduler thread too).
+        self._stalls = []          # (ms, what)
+        self._gc_pauses = []       # (generation, ms)
+        self._gc_t0 = None
+        if freeze_gc:
+            # A full collection traverses every tracked object of the process
+            # (with torch loaded: hundreds of thousands, ~0.1 s).  Objects that
+            # exist when the server starts are long-lived, so move them out of
+            # the collector's generations; collections while serving then
+            # traverse only what was made since.  Process-wide, as Python's
+            # gc.freeze is.
+            gc.collect()
+            gc.freeze()
+        gc.callbacks.append(self._on_gc)
         self._thread = threading.Thread(target=self._loop, name="gsmc-serve", daemon=True)
         self._thread.start()
 
@@ -227,12 +245,30 @@ class TmrcaServer:
             self._cv.notify()
         return fut
 
+    def _on_gc(self, phase, info):
+        if phase == "start":
+            self._gc_t0 = time.perf_counter()
+        elif self._gc_t0 is not None:
+            ms = (time.perf_counter() - self._gc_t0) * 1e3
+            self._gc_t0 = None
+            if ms >= 1.0 and len(self._gc_pauses) < 10000:
+                self._gc_pauses.append((int(info.get("generation", -1)), ms))
+
+    def _note_stall(self, t0, what):
+        ms = (time.perf_counter() - t0) * 1e3
+        if ms >= 2.0 and len(self._stalls) < 10000:
+            self._stalls.append((ms, what))
+
     def close(self, wait=True):
         with self._cv:
             self._closing = True
             self._cv.notify()
         if wait:
             self._thread.join()
+        try:
+            gc.callbacks.remove(self._on_gc)
+        except ValueError:
+            pass
         for s in self.slots:
             s.executor.close()
         if self._redo_ex is not None:
@@ -249,10 +285,17 @@ class TmrcaServer:
         with self._cv:
             done = list(self._done)
             counters = dict(self.counters)
+            stalls, pauses = list(self._stalls), list(self._gc_pauses)
             if reset:
                 self._done.clear()
                 self.counters.clear()
+                self._stalls.clear()
+                self._gc_pauses.clear()
         out = {"completed": len(done), **counters}
+        # longest scheduler stalls and collector pauses (>= 2 ms / >= 1 ms)
+        out["loop_stalls_ms"] = [(round(ms, 2), what) for ms, what in sorted(stalls)[-5:][::-1]]
+        out["gc_pauses"] = len(pauses)
+        out["gc_max_ms"] = max((ms for _, ms in pauses), default=0.0)
         if done:
             t = np.array(done)
             lat = (t[:, 2] - t[:, 0]) * 1e3
@@ -354,11 +397,14 @@ class TmrcaServer:
                              or ntasks + req.tasks > self.max_tasks
                              or work + req.job.pair_sites > self.max_batch_pair_sites
                              or (cap is not None and nbytes + req.bytes > cap)):
-                    break
+                    break   # the batch is full; the rest go to the next free executor
+                # why the head query waits (counted once per admission pass)
                 if self._in_use + req.bytes > self.hbm_budget:
+                    self.counters["wait_hbm"] += 1
                     break
                 if (not take and cap is not None and req.bytes > cap and in_flight
                         and req.bytes <= self.arena.size):
+                    self.counters["wait_arena"] += 1
                     break
                 self._pending.popleft()
                 take.append(req)
@@ -397,11 +443,19 @@ class TmrcaServer:
             busy = False
             for slot in self.slots:
                 if slot.batch is not None and slot.batch.done.query():
+                    t0 = time.perf_counter()
                     self._finish(slot)
+                    self._note_stall(t0, "finish")
                     busy = True
+            free = False
             for slot in self.slots:
                 if slot.batch is None and self._pending:
+                    free = True
+                    t0 = time.perf_counter()
                     busy |= self._admit(slot)
+                    self._note_stall(t0, "admit")
+            if self._pending and not free:
+                self.counters["wait_executor"] += 1
             with self._cv:
                 idle = all(s.batch is None for s in self.slots)
                 if self._closing and not self._pending and idle:

@@ -443,6 +443,22 @@ int gsmc_ctx_tables_info(const gsmc_ctx* ctx, double* build_seconds, int* reused
 int gsmc_free_cached_tables(void);
 
 /*
+ * Page-locked host buffers for results, cached for reuse.  A host output
+ * array that is page-locked is written by the device-to-host DMA directly
+ * (no staging ring, no host thread touching the data), which is what repeated
+ * large calls want; allocating page-locked memory is slow (seconds per 100
+ * GB), so released buffers are kept and handed out again to requests they fit
+ * (at most twice the request).  gsmc_host_free returns a buffer to the cache;
+ * gsmc_host_cache_limit bounds the bytes kept cached (default 256 GiB;
+ * 0 frees every cached buffer).  No reference counterpart (the reference
+ * pins its fresh output arrays with cudaHostRegister on every call,
+ * src/bindings.cpp:3086-3092).
+ */
+int gsmc_host_alloc(uint64_t bytes, void** ptr);
+int gsmc_host_free(void* ptr);
+int gsmc_host_cache_limit(uint64_t max_cached_bytes);
+
+/*
  * Poll budget of the uncached kernels' wait for their shared-memory copy of
  * the flow field (default 2^24 mbarrier polls, process-wide, read at each
  * gsmc_flow_fb call).  A CTA whose copy has not landed within the budget

@@ -285,3 +285,26 @@ def test_collection_failure_fails_only_its_batch(server_factory):
     _check_result(s.submit([(3, 1)], 10, 60), 3, 10, 60, 1, ("mean",))
     st = s.stats()
     assert st["failed"] >= 1 and st["completed"] >= 1
+
+
+def test_tail_diagnostics(server_factory):
+    """The server reports why queries waited (no free executor, HBM budget),
+    its longest scheduler stalls and the collector's pauses while serving."""
+    import gc
+    s, rec = server_factory(max_inflight=1, hbm_budget=4 * 500 * 20)
+    rec.delay = 0.02
+    futs = [s.submit([(1, 0)], 0, 500)]
+    time.sleep(0.005)   # the first query's batch is on the (only) executor now
+    futs += [s.submit([(1 + (i % 19), 0)], 0, 500) for i in range(5)]
+    for f in futs:
+        f.result(timeout=10)
+    gc.collect()   # a collection while the server runs is recorded (>= 1 ms only)
+    st = s.stats()
+    assert st["wait_executor"] > 0            # one executor: the others queued behind it
+    assert isinstance(st["loop_stalls_ms"], list) and isinstance(st["gc_pauses"], int)
+    assert st["gc_max_ms"] >= 0.0
+    s2, _ = server_factory(max_inflight=2, hbm_budget=6000)   # room for one query
+    fa = [s2.submit([(1, 0), (2, 0)], 0, 500) for _ in range(3)]
+    for f in fa:
+        f.result(timeout=10)
+    assert s2.stats()["wait_hbm"] > 0

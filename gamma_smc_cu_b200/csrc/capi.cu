@@ -410,27 +410,29 @@ int resident_ctas(ScanShape shape) {
 
 int spec_chunks(const gsmc_ctx* ctx, int64_t tasks, int64_t resident_tiles, int64_t core_len,
                 int flags);
+double launch_cost(int64_t n, int64_t r, double steps);
+double chunk_steps(int64_t core_len, int K, int64_t b);
+int64_t max_core(const std::vector<Block>& blocks);
 
 // Launch shape of a call over P pairs x `blocks`: two pairs per thread (two
-// independent lookup chains per thread; 6-8% faster) when that still gives
-// every resident CTA two (window, pair tile) tasks, or at least one once
-// the windows are cut into speculative chunks; else one pair per thread (twice
-// the tasks, for calls too small to fill the GPU either way).
+// independent lookup chains per thread; 6-8% faster per pair) when that
+// gives every resident CTA two (window, pair tile) tasks; otherwise the shape
+// whose best speculative chunking has the lower launch_cost, a two-pair tile
+// task taking 1.45 times a one-pair one (twice the pairs per thread, 8
+// instead of 10 resident CTAs per SM, 10% faster per pair).
 void pick_shape(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int flags) {
   if (ctx->shape_fixed) return;
-  const ScanShape two{scan_threads(), 2};
-  const int64_t tiles = ceil_div(P, scan_tile_pairs(two));
-  const int64_t tasks = (int64_t)blocks.size() * tiles;
-  const int64_t resident = resident_ctas(two);
-  bool use_two = tasks >= 2 * resident;
-  if (!use_two) {
-    int64_t chunked = 0;
-    for (const Block& b : blocks)
-      chunked += tiles * spec_chunks(ctx, tasks, resident * scan_tiles_per_cta(two), b.ce - b.cs,
-                                     flags);
-    use_two = chunked >= resident;
-  }
-  ctx->shape = use_two ? two : ScanShape{scan_threads(), 1};
+  const ScanShape two{scan_threads(), 2}, one{scan_threads(), 1};
+  const int64_t core = max_core(blocks);
+  auto cost = [&](ScanShape sh, double per_step) {
+    const int64_t tasks = (int64_t)blocks.size() * ceil_div(P, scan_tile_pairs(sh));
+    const int64_t tiles = (int64_t)resident_ctas(sh) * scan_tiles_per_cta(sh);
+    const int K = spec_chunks(ctx, tasks, tiles, core, flags);
+    return per_step * launch_cost(tasks * K, tiles, chunk_steps(core, K, ctx->spec_flank));
+  };
+  const int64_t tasks2 = (int64_t)blocks.size() * ceil_div(P, scan_tile_pairs(two));
+  const bool use_two = tasks2 >= 2 * resident_ctas(two) || cost(two, 1.45) <= cost(one, 1.0);
+  ctx->shape = use_two ? two : one;
 }
 
 // Pair-steps of a task per pair: forward over [ps, ce), backward over [cs, pe).
@@ -578,16 +580,49 @@ struct SpecLaunch {
   int64_t max_core = 0;             // longest whole core (repair slot rows)
 };
 
+// Estimated duration, in pair-steps of one tile, of a persistent launch of n
+// equal tasks of `steps` pair-steps each on r resident tiles: full waves of r
+// tasks, and a partial last wave that runs faster (fewer CTAs share the SMs)
+// but not in proportion to its size -- modelled as max(fraction, 0.8) of a
+// full wave (on the 50,000-site full-posterior slice, 63,190 pairs: 988
+// tasks on 1,184 tiles took 42 ms, 1,482 took 50 ms, 1,235 took 55 ms).
+double launch_cost(int64_t n, int64_t r, double steps) {
+  if (n <= 0 || r <= 0) return 0.0;
+  const int64_t full = n / r;
+  const double frac = (double)(n % r) / (double)r;
+  return steps * ((double)full + (frac > 0.0 ? std::max(frac, 0.8) : 0.0));
+}
+
+// Longest task (pair-steps per pair) of a core of core_len sites cut into K
+// chunks with burn-in b: each interior boundary adds b forward steps to the
+// right chunk and b backward steps to the left one.
+double chunk_steps(int64_t core_len, int K, int64_t b) {
+  const double c = (double)ceil_div(core_len, K);
+  return 2.0 * c + (K >= 3 ? 2.0 * b : K == 2 ? (double)b : 0.0);
+}
+
 // Chunks per window for a launch of `tasks` tasks on `resident_tiles`
-// tiles: about twice the tiles, chunks of at least kSpecMinCore sites.
+// tiles: none when the tasks fill the GPU twice; otherwise the K (chunks of
+// at least two burn-ins) that minimises launch_cost -- balancing the
+// burn-in steps each extra chunk adds against filling the last wave.
 int spec_chunks(const gsmc_ctx* ctx, int64_t tasks, int64_t resident_tiles, int64_t core_len,
                 int flags) {
   if (!ctx->speculate || (flags & kTaskSummary) || tasks <= 0) return 1;
   if (ctx->spec_chunks_fixed > 0)
     return (int)std::max<int64_t>(1, std::min<int64_t>(ctx->spec_chunks_fixed, core_len / 64));
   if (tasks >= 2 * resident_tiles) return 1;
-  const int64_t want = ceil_div(2 * resident_tiles, tasks);
-  return (int)std::max<int64_t>(1, std::min<int64_t>(want, core_len / (4 * ctx->spec_flank)));
+  const int64_t b = ctx->spec_flank;
+  const int k_max = (int)std::max<int64_t>(1, std::min<int64_t>(1024, core_len / (2 * b)));
+  int best = 1;
+  double best_cost = launch_cost(tasks, resident_tiles, chunk_steps(core_len, 1, b));
+  for (int K = 2; K <= k_max; ++K) {
+    const double c = launch_cost(tasks * K, resident_tiles, chunk_steps(core_len, K, b));
+    if (c < best_cost * 0.999) {
+      best = K;
+      best_cost = c;
+    }
+  }
+  return best;
 }
 
 // Append the tasks of window b for the n pairs at (pi, pj): whole, or in K

@@ -2047,8 +2047,8 @@ int gsmc_ctx_table_layer(const gsmc_ctx* ctx, int table, int layer, float* out) 
       const int pr = std::min(r, kPatchRows - 1), pq = std::min(q, kPatchCols - 1);
       const int corner = (r - pr) * 2 + (q - pq);
       const float* p = patches.data() + (size_t)(pr * kPatchCols + pq) * 8;
-      out[r * kCols + q] = p[2 * corner];
-      out[kCells + r * kCols + q] = p[2 * corner + 1];
+      out[r * kCols + q] = p[corner];
+      out[kCells + r * kCols + q] = p[4 + corner];
     }
   return GSMC_OK;
 }

@@ -23,6 +23,28 @@ constexpr float kCStep = (kCHi - kCLo) / (kCols - 1);
 constexpr float kMInv = 1.0f / kMStep;
 constexpr float kCInv = 1.0f / kCStep;
 
+// Bilinear lookup of (m, c) in one patch layer, identical to the reference's
+// clamp / truncate / keep-the-upper-cell interpolation.  Split in two so
+// independent work can be scheduled between the loads and their use.
+struct Fetch {
+  float4 a, b;  // m corners and c corners of the patch
+  float wm, wc;
+  int idx;      // patch index within the layer
+};
+
+// Hint the patch a pair will most likely read at its next site (same cell,
+// next site's layer, next site's hom/het half) into L1.  Compiled only with
+// GSMC_PREFETCH_NEXT: on the chromosome job the extra instructions cost more
+// than the hits gained (304 ms against 282 ms per job when measured), so the
+// default build emits nothing here.
+__device__ __forceinline__ void prefetch_patch(const float4* p) {
+#ifdef GSMC_PREFETCH_NEXT
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+#else
+  (void)p;
+#endif
+}
+
 // floor(x) for 0 <= x < 2^23 in two full-rate adds: x + 2^23 lands in
 // [2^23, 2^24), where floats are the integers, and rounding the sum down keeps
 // 2^23 + floor(x) exactly.
@@ -30,142 +52,59 @@ __device__ __forceinline__ float floor_small(float x) {
   return __fsub_rn(__fadd_rd(x, 8388608.0f), 8388608.0f);
 }
 
-// Two float32 lanes in one 64-bit register pair, the operands of sm_100's
-// packed FP32 instructions (add/sub/mul/fma.rn.f32x2).  Each lane is rounded
-// exactly as the scalar instruction rounds it, so the packed arithmetic below
-// is bit-identical to the scalar expressions it stands for, at one issued
-// instruction where the scalar form needs two.  The scan state is such a
-// pair: lo = log10 mean m, hi = log10 CV c.
-struct f2 {
-  unsigned long long v;
-};
-
-__device__ __forceinline__ f2 pack2(float lo, float hi) {
-  f2 r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(lo), "f"(hi));
-  return r;
-}
-__device__ __forceinline__ float lo_of(f2 a) {
-  float lo, hi;
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a.v));
-  return lo;
-}
-__device__ __forceinline__ float hi_of(f2 a) {
-  float lo, hi;
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a.v));
-  return hi;
-}
-__device__ __forceinline__ f2 add2(f2 a, f2 b) {
-  f2 r;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
-  return r;
-}
-// rounded toward -infinity (the packed floor_small)
-__device__ __forceinline__ f2 add2_rd(f2 a, f2 b) {
-  f2 r;
-  asm("add.rm.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
-  return r;
-}
-__device__ __forceinline__ f2 sub2(f2 a, f2 b) {
-  f2 r;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
-  return r;
-}
-__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
-  f2 r;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
-  return r;
-}
-__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
-  f2 r;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
-  return r;
-}
-__device__ __forceinline__ f2 as_f2(float2 v) { return pack2(v.x, v.y); }
-__device__ __forceinline__ float2 as_float2(f2 v) { return make_float2(lo_of(v), hi_of(v)); }
-
-// Bilinear lookup of a state (m, c) in one patch layer, identical to the
-// reference's clamp / truncate / keep-the-upper-cell interpolation
-// (src/kernels/gamma_smc_flow.cu:408-431).  Split in two so independent work
-// can be scheduled between the load and its use.
-struct Fetch {
-  f2 p00, p01, p10, p11;  // (m, c) at corners (r,q) (r,q+1) (r+1,q) (r+1,q+1)
-  f2 w;                   // {wm, wc}: weights of the upper row / column
-};
-
-// 49 * bits(2^23 + r) + bits(2^23 + q) = 49 r + q + kIdxBias (mod 2^32); see
-// patch_fetch.
-constexpr unsigned kIdxBias = 50u * 0x4B000000u;
-
-__device__ __forceinline__ Fetch patch_fetch(const float4* __restrict__ layer, f2 s) {
-  const f2 f = mul2(sub2(s, pack2(kMLo, kCLo)), pack2(kMInv, kCInv));
-  const float fm = fmaxf(0.0f, fminf(lo_of(f), (float)(kRows - 1)));
-  const float fc = fmaxf(0.0f, fminf(hi_of(f), (float)(kCols - 1)));
+__device__ __forceinline__ Fetch patch_fetch(const float4* __restrict__ layer, float m, float c) {
+  float fm = __fmul_rn(__fsub_rn(m, kMLo), kMInv);
+  float fc = __fmul_rn(__fsub_rn(c, kCLo), kCInv);
+  fm = fmaxf(0.0f, fminf(fm, (float)(kRows - 1)));
+  fc = fmaxf(0.0f, fminf(fc, (float)(kCols - 1)));
   // Lower-left corner: the reference truncates (fm >= 0, so floor) and moves
   // an index that lands on the last row/column down by one.  floor(min(x,
   // last - 0.5)) is both at once, and the weight stays x - corner.
-  const f2 k23 = pack2(8388608.0f, 8388608.0f);
-  const f2 big = add2_rd(pack2(fminf(fm, (float)kPatchRows - 0.5f),
-                               fminf(fc, (float)kPatchCols - 0.5f)), k23);
-  Fetch r;
-  r.w = sub2(pack2(fm, fc), sub2(big, k23));
-  // The bits of 2^23 + k are 0x4B000000 + k, so 49 * bits(2^23 + rf) +
-  // bits(2^23 + qf) is the patch index rf * 49 + qf (< 2450) plus
-  // 50 * 0x4B000000 mod 2^32 = 0xA6000000, with no further wrap: the index in
-  // one integer multiply-add, its bias folded into the layer address.
-  const unsigned t =
-      __float_as_uint(lo_of(big)) * (unsigned)kPatchCols + __float_as_uint(hi_of(big));
-  const unsigned long long addr = reinterpret_cast<unsigned long long>(layer) -
-                                  (unsigned long long)kIdxBias * 32ull +
-                                  (unsigned long long)t * 32ull;
-  // One 256-bit read-only load of the 32-byte patch into four (m, c) pairs.
-  // Patches are 32-byte aligned: table bases come from cudaMalloc and every
-  // layer, hom/het half and patch offset is a multiple of 32 bytes.
-  asm("ld.global.nc.v4.b64 {%0, %1, %2, %3}, [%4];"
-      : "=l"(r.p00.v), "=l"(r.p01.v), "=l"(r.p10.v), "=l"(r.p11.v)
-      : "l"(addr));
-  return r;
+  const float rf = floor_small(fminf(fm, (float)kPatchRows - 0.5f));
+  const float qf = floor_small(fminf(fc, (float)kPatchCols - 0.5f));
+  Fetch f;
+  f.wm = __fsub_rn(fm, rf);
+  f.wc = __fsub_rn(fc, qf);
+  // rf * 49 + qf is an exact integer below 2450; adding 2^23 places it in the
+  // low mantissa bits, so the patch index needs no conversion instruction.
+  const int idx = __float_as_int(__fadd_rn(__fmaf_rn(rf, (float)kPatchCols, qf), 8388608.0f)) -
+                  0x4B000000;
+  // One 256-bit read-only load of the 32-byte patch: m corners (r,q) (r,q+1)
+  // (r+1,q) (r+1,q+1), then the c corners.  Patches are 32-byte aligned:
+  // table bases come from cudaMalloc and every layer, hom/het half and patch
+  // offset is a multiple of 32 bytes.
+  f.idx = idx;
+  const float4* p = layer + kPatchF4 * idx;
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(f.a.x), "=f"(f.a.y), "=f"(f.a.z), "=f"(f.a.w), "=f"(f.b.x), "=f"(f.b.y),
+        "=f"(f.b.z), "=f"(f.b.w)
+      : "l"(p));
+  return f;
 }
 
-// m = fma(wm, fma(wc, m11, vc * m10), vm * fma(wc, m01, vc * m00)), and the
-// same for c, with vm = 1 - wm, vc = 1 - wc: both lanes at once.
-__device__ __forceinline__ f2 patch_interp(const Fetch& f) {
-  const f2 v = sub2(pack2(1.0f, 1.0f), f.w);
-  const float wm = lo_of(f.w), wc = hi_of(f.w), vm = lo_of(v), vc = hi_of(v);
-  const f2 wc2 = pack2(wc, wc), vc2 = pack2(vc, vc);
-  const f2 hi_row = fma2(wc2, f.p11, mul2(vc2, f.p10));
-  const f2 lo_row = fma2(wc2, f.p01, mul2(vc2, f.p00));
-  return fma2(pack2(wm, wm), hi_row, mul2(pack2(vm, vm), lo_row));
+__device__ __forceinline__ void patch_interp(const Fetch& f, float& m, float& c) {
+  const float vc = __fsub_rn(1.0f, f.wc), vm = __fsub_rn(1.0f, f.wm);
+  m = __fmaf_rn(f.wm, __fmaf_rn(f.wc, f.a.w, __fmul_rn(vc, f.a.z)),
+                __fmul_rn(vm, __fmaf_rn(f.wc, f.a.y, __fmul_rn(vc, f.a.x))));
+  c = __fmaf_rn(f.wm, __fmaf_rn(f.wc, f.b.w, __fmul_rn(vc, f.b.z)),
+                __fmul_rn(vm, __fmaf_rn(f.wc, f.b.y, __fmul_rn(vc, f.b.x))));
 }
 
-__device__ __forceinline__ f2 patch_lookup(const float4* __restrict__ layer, f2 s) {
-  return patch_interp(patch_fetch(layer, s));
+__device__ __forceinline__ void patch_lookup(const float4* __restrict__ layer, float& m,
+                                             float& c) {
+  const Fetch f = patch_fetch(layer, m, c);
+  patch_interp(f, m, c);
 }
 
 // 10^x by the bit construction upstream gamma_smc uses (Schraudolph 1999,
 // "A fast, compact approximation of the exponential function"): the float
 // whose bits are trunc(C2 * (x * ln10) + C1) (src/kernels/gamma_smc_flow.cu:
 // 112-121).
-constexpr float kLn10 = 2.30258509299f;
-constexpr float kPowC1 = 1064872507.1541044f;
-constexpr float kPowC2 = 12102203.161561485f;
-
 __device__ __forceinline__ float pow10_bits(float x) {
-  return __int_as_float(__float2int_rz(__fmaf_rn(kPowC2, __fmul_rn(x, kLn10), kPowC1)));
-}
-
-// Two arguments at once: the multiply and the multiply-add packed, the
-// truncations one by one.
-__device__ __forceinline__ f2 pow10_bits2(f2 x) {
-  const f2 y = fma2(pack2(kPowC2, kPowC2), mul2(x, pack2(kLn10, kLn10)), pack2(kPowC1, kPowC1));
-  return pack2(__int_as_float(__float2int_rz(lo_of(y))), __int_as_float(__float2int_rz(hi_of(y))));
-}
-
-// {10^(-2c), 10^(-2c - m)}: a state's Gamma shape and rate terms
-// (mc_to_ab, src/kernels/gamma_smc_flow.cu:123-131).
-__device__ __forceinline__ f2 mc_to_ab(f2 s) {
-  const float a = -2.0f * hi_of(s);
-  return pow10_bits2(pack2(a, __fsub_rn(a, lo_of(s))));
+  const float kLn10 = 2.30258509299f;
+  const float kC1 = 1064872507.1541044f;
+  const float kC2 = 12102203.161561485f;
+  return __int_as_float(__float2int_rz(__fmaf_rn(kC2, __fmul_rn(x, kLn10), kC1)));
 }
 
 __device__ __forceinline__ uint64_t word_at(const ulonglong2* g, int64_t nh, int s) {
@@ -173,22 +112,25 @@ __device__ __forceinline__ uint64_t word_at(const ulonglong2* g, int64_t nh, int
   return (s & 64) ? v.y : v.x;
 }
 
-// Posterior at one core site from the forward state f and the backward state
-// b (src/kernels/gamma_smc_flow.cu:708-722): alpha = af + ab - 1,
-// beta = bf + bb - 1, mean = alpha / max(beta, 1e-10) * 2 Ne.
-__device__ __forceinline__ float posterior(f2 f, f2 b, float unscale, float& a_s, float& b_s) {
-  const f2 ab = sub2(add2(mc_to_ab(f), mc_to_ab(b)), pack2(1.0f, 1.0f));
-  a_s = lo_of(ab);
-  b_s = hi_of(ab);
+// Posterior at one core site: forward state f, backward state (m, c) ->
+// alpha, beta and the mean in generations (src/kernels/gamma_smc_flow.cu:708-722).
+__device__ __forceinline__ float posterior(float2 f, float m, float c, float unscale, float& a_s,
+                                           float& b_s) {
+  const float ab = -2.0f * c;
+  const float ba = pow10_bits(ab), bb = pow10_bits(__fsub_rn(ab, m));
+  const float af = -2.0f * f.y;
+  const float fa = pow10_bits(af), fb = pow10_bits(__fsub_rn(af, f.x));
+  a_s = __fsub_rn(__fadd_rn(fa, ba), 1.0f);
+  b_s = __fsub_rn(__fadd_rn(fb, bb), 1.0f);
   return __fmul_rn(__fdiv_rn(a_s, fmaxf(b_s, 1e-10f)), unscale);
 }
 
 // Posterior combine at one core site, stored per pair
 // (src/kernels/gamma_smc_flow.cu:708-734).
-__device__ __forceinline__ void combine_store(const Task& t, int64_t o, f2 f, f2 b, bool ci,
-                                              bool post) {
+__device__ __forceinline__ void combine_store(const Task& t, int64_t o, float2 f, float m, float c,
+                                              bool ci, bool post) {
   float a_s, b_s;
-  const float mg = posterior(f, b, t.unscale, a_s, b_s);
+  const float mg = posterior(f, m, c, t.unscale, a_s, b_s);
   __stcs(t.out[0] + o, mg);
   if (ci) {
     // Wilson-Hilferty 95% bounds (src/kernels/gamma_smc_flow.cu:724-733).
@@ -204,12 +146,6 @@ __device__ __forceinline__ void combine_store(const Task& t, int64_t o, f2 f, f2
     __stcs(t.out[3] + o, a_s);
     __stcs(t.out[4] + o, b_s);
   }
-}
-
-// The same from scalar states (the uncached kernels).
-__device__ __forceinline__ void combine_store(const Task& t, int64_t o, float2 f, float m, float c,
-                                              bool ci, bool post) {
-  combine_store(t, o, as_f2(f), pack2(m, c), ci, post);
 }
 
 // Forward states are read back this many sites ahead of their use so the
@@ -269,15 +205,17 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   const float4* __restrict__ chunk = a.chunk_tab;
 
   // ---- forward: [ps, ce); states stored for [cs, ce) ----
-  f2 st[NP];
+  float m[NP], c[NP];
   uint32_t x[NP];
 #pragma unroll
   for (int k = 0; k < NP; ++k) {
-    st[k] = pack2(0.0f, 0.0f);
+    m[k] = 0.0f;
+    c[k] = 0.0f;
     x[k] = (uint32_t)((word_at(gi[k], nh, ps) ^ word_at(gj[k], nh, ps)) >> (ps & 63));
   }
   float2* fp = slot + j0;
-  // Gap codes run two sites ahead: `cur` is this site's, `nx` the next one's.
+  // Gap codes run two sites ahead: `cur` is this site's, `nx` the next one's
+  // (already in registers, so the next-site prefetch does not wait on it).
   // het bits: 32-bit halves of the pair's XORed genotype words (a 32-bit
   // shift per site); the loops below run in 32-site blocks and reload at each
   // block's first site (the first site of the task comes preloaded)
@@ -286,11 +224,11 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     for (int k = 0; k < NP; ++k)
       x[k] = (uint32_t)((word_at(gi[k], nh, s) ^ word_at(gj[k], nh, s)) >> (s & 32));
   };
-  auto fwd_step = [&](SiteCode sc) {
+  auto fwd_step = [&](int s, SiteCode sc, int next_layer) {
     if (sc.chunks) {
       for (int u = 0; u < sc.chunks; ++u) {
 #pragma unroll
-        for (int k = 0; k < NP; ++k) st[k] = patch_lookup(chunk, st[k]);
+        for (int k = 0; k < NP; ++k) patch_lookup(chunk, m[k], c[k]);
       }
     }
     const float4* layer = fwd_tab + sc.layer;
@@ -299,10 +237,11 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     for (int k = 0; k < NP; ++k) {
       const int het = (int)(x[k] & 1u);
       x[k] >>= 1;
-      f[k] = patch_fetch(layer + het * kHetF4, st[k]);
+      f[k] = patch_fetch(layer + het * kHetF4, m[k], c[k]);
+      prefetch_patch(fwd_tab + next_layer + (int)(x[k] & 1u) * kHetF4 + kPatchF4 * f[k].idx);
     }
 #pragma unroll
-    for (int k = 0; k < NP; ++k) st[k] = patch_interp(f[k]);
+    for (int k = 0; k < NP; ++k) patch_interp(f[k], m[k], c[k]);
   };
   int s = ps;
   // a window that does not start at site 0 enters its first site by 1 bp
@@ -310,20 +249,20 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   SiteCode nx = code[s + 1];
   {
     const SiteCode nx2 = code[s + 2];
-    fwd_step(cur);
+    fwd_step(s, cur, nx.layer);
     cur = nx;
     nx = nx2;
   }
   if (s >= cs) {
 #pragma unroll
-    for (int k = 0; k < NP; ++k) __stcs(fp + k * WIDTH, as_float2(st[k]));
+    for (int k = 0; k < NP; ++k) __stcs(fp + k * WIDTH, make_float2(m[k], c[k]));
     fp += kRow;
   }
   for (++s; s < cs;) {
     if ((s & 31) == 0) reload(s);
     for (const int e = min(cs, (s | 31) + 1); s < e; ++s) {
       const SiteCode nx2 = code[s + 2];
-      fwd_step(cur);
+      fwd_step(s, cur, nx.layer);
       cur = nx;
       nx = nx2;
     }
@@ -334,7 +273,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
       const int j = j0 + k * WIDTH;
-      if (j < t.pair_count) b[kind * t.bstride + j] = as_float2(st[k]);
+      if (j < t.pair_count) b[kind * t.bstride + j] = make_float2(m[k], c[k]);
     }
   };
   if (t.bl) record(t.bl, 1);
@@ -342,11 +281,11 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     if ((s & 31) == 0 && s != ps) reload(s);
     for (const int e = min(ce, (s | 31) + 1); s < e; ++s) {
       const SiteCode nx2 = code[s + 2];
-      fwd_step(cur);
+      fwd_step(s, cur, nx.layer);
       cur = nx;
       nx = nx2;
 #pragma unroll
-      for (int k = 0; k < NP; ++k) __stcs(fp + k * WIDTH, as_float2(st[k]));
+      for (int k = 0; k < NP; ++k) __stcs(fp + k * WIDTH, make_float2(m[k], c[k]));
       fp += kRow;
     }
   }
@@ -355,28 +294,30 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   // ---- backward: [pe-1 .. cs]; posterior at core sites ----
 #pragma unroll
   for (int k = 0; k < NP; ++k) {
-    st[k] = pack2(0.0f, 0.0f);
+    m[k] = 0.0f;
+    c[k] = 0.0f;
     x[k] = (uint32_t)((word_at(gi[k], nh, pe - 1) ^ word_at(gj[k], nh, pe - 1)) >> ((pe - 1) & 32))
            << (31 - ((pe - 1) & 31));
   }
   // Backward step at site s: the het/hom site table first, then any full
   // 1000-bp chunks.
-  auto bwd_fetch = [&](SiteCode sc, Fetch* f) {
+  auto bwd_fetch = [&](int s, SiteCode sc, int next_layer, Fetch* f) {
     const float4* layer = bwd_tab + sc.layer;
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
       const int het = (int)(x[k] >> 31);
       x[k] <<= 1;
-      f[k] = patch_fetch(layer + het * kHetF4, st[k]);
+      f[k] = patch_fetch(layer + het * kHetF4, m[k], c[k]);
+      prefetch_patch(bwd_tab + next_layer + (int)(x[k] >> 31) * kHetF4 + kPatchF4 * f[k].idx);
     }
   };
   auto bwd_finish = [&](SiteCode sc, const Fetch* f) {
 #pragma unroll
-    for (int k = 0; k < NP; ++k) st[k] = patch_interp(f[k]);
+    for (int k = 0; k < NP; ++k) patch_interp(f[k], m[k], c[k]);
     if (sc.chunks) {
       for (int u = 0; u < sc.chunks; ++u) {
 #pragma unroll
-        for (int k = 0; k < NP; ++k) st[k] = patch_lookup(chunk, st[k]);
+        for (int k = 0; k < NP; ++k) patch_lookup(chunk, m[k], c[k]);
       }
     }
   };
@@ -388,7 +329,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     for (const int e = max(ce, s & ~31); s >= e; --s) {
       const SiteCode nx2 = code[s - 2];
       Fetch f[NP];
-      bwd_fetch(cur, f);
+      bwd_fetch(s, cur, nx.layer, f);
       bwd_finish(cur, f);
       cur = nx;
       nx = nx2;
@@ -397,12 +338,12 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   if (t.br) record(t.br, 3);
   // forward-state ring: q[i] holds the state of site s - i
   const float2* fq = slot + (int64_t)(ce - 1 - cs) * kRow + j0;
-  f2 q[kFwdPrefetch][NP];
+  float2 q[kFwdPrefetch][NP];
 #pragma unroll
   for (int i = 0; i < kFwdPrefetch; ++i) {
 #pragma unroll
     for (int k = 0; k < NP; ++k)
-      q[i][k] = (ce - 1 - i >= cs) ? as_f2(__ldlu(fq + k * WIDTH)) : pack2(0.0f, 0.0f);
+      q[i][k] = (ce - 1 - i >= cs) ? __ldlu(fq + k * WIDTH) : make_float2(0.0f, 0.0f);
     fq -= kRow;
   }
   int64_t o = t.out_off + (int64_t)(ce - 1 - t.out_row0) * t.ldo + j0;
@@ -412,7 +353,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   // unrolled by the ring depth so the ring rotation is register renaming
 #pragma unroll kFwdPrefetch
   for (const int e = max(cs, s & ~31); s >= e; --s) {
-    f2 f[NP];
+    float2 f[NP];
 #pragma unroll
     for (int k = 0; k < NP; ++k) f[k] = q[0][k];
 #pragma unroll
@@ -423,10 +364,16 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     const bool ahead = s - kFwdPrefetch >= cs;
 #pragma unroll
     for (int k = 0; k < NP; ++k)
-      q[kFwdPrefetch - 1][k] = ahead ? as_f2(__ldlu(fq + k * WIDTH)) : pack2(0.0f, 0.0f);
+      q[kFwdPrefetch - 1][k] = ahead ? __ldlu(fq + k * WIDTH) : make_float2(0.0f, 0.0f);
     fq -= kRow;
     const SiteCode sc = cur;
     const SiteCode nx2 = code[s - 2];
+    float mb[NP], cb[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      mb[k] = m[k];
+      cb[k] = c[k];
+    }
     const bool more = s > cs;
     // The combine runs before the next lookup is issued: holding the patch
     // registers across it costs more occupancy than the overlap gains.
@@ -437,7 +384,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
 #pragma unroll
       for (int k = 0; k < NP; ++k) {
         float a_s, b_s;
-        const float mg = posterior(f[k], st[k], t.unscale, a_s, b_s);
+        const float mg = posterior(f[k], mb[k], cb[k], t.unscale, a_s, b_s);
         if (live[k]) {
           vs = __fadd_rn(vs, mg);
           vmin = fminf(vmin, mg);
@@ -459,12 +406,12 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     } else {
 #pragma unroll
       for (int k = 0; k < NP; ++k)
-        if (live[k]) combine_store(t, o + k * WIDTH, f[k], st[k], ci, post);
+        if (live[k]) combine_store(t, o + k * WIDTH, f[k], mb[k], cb[k], ci, post);
     }
     o -= t.ldo;
     if (more) {
       Fetch fe[NP];
-      bwd_fetch(sc, fe);
+      bwd_fetch(s, sc, nx.layer, fe);
       bwd_finish(sc, fe);
     }
     cur = nx;
@@ -475,7 +422,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     // the backward state after applying site cs itself, for the left neighbour
     Fetch fe[NP];
     const SiteCode scs = code[cs];
-    bwd_fetch(scs, fe);
+    bwd_fetch(cs, scs, 0, fe);
     bwd_finish(scs, fe);
     record(t.bl, 2);
   }

@@ -299,10 +299,11 @@ void scaled_rates(double Ne, double mu, double rho, float* scaled_rho, float* sc
   *scaled_mu = 4.0f * ne * (float)mu;
 }
 
-// Planar patch: one 8-value patch per interpolation cell (r, q), r < 50,
+// Scan layout: one 32-byte patch per interpolation cell (r, q), r < 50,
 // q < 49, holding the four corners of m then of c:
 //   {m[r][q], m[r][q+1], m[r+1][q], m[r+1][q+1]}, {c[r][q], ..., c[r+1][q+1]}
-// (the forward-only path's half-precision table converts this layout).
+// so one lookup is a single 256-bit load of one 32-byte sector (the
+// forward-only path's half-precision table converts the same layout).
 void pack_patches(const float* m, const float* c, float* dst) {
   for (int r = 0; r < kPatchRows; ++r)
     for (int q = 0; q < kPatchCols; ++q) {
@@ -312,24 +313,6 @@ void pack_patches(const float* m, const float* c, float* dst) {
       for (int k = 0; k < 4; ++k) {
         p[k] = m[corner[k]];
         p[4 + k] = c[corner[k]];
-      }
-    }
-}
-
-// Scan layout: one 32-byte patch per interpolation cell (r, q), r < 50,
-// q < 49, holding the (m, c) pair of each corner:
-//   {m, c}[r][q], {m, c}[r][q+1], {m, c}[r+1][q], {m, c}[r+1][q+1]
-// so one lookup is a single 256-bit load whose four 64-bit quarters are the
-// packed (m, c) operands of the scan's two-lane interpolation.
-void pack_patches_mc(const float* m, const float* c, float* dst) {
-  for (int r = 0; r < kPatchRows; ++r)
-    for (int q = 0; q < kPatchCols; ++q) {
-      const int a = r * kCols + q;
-      const int corner[4] = {a, a + 1, a + kCols, a + kCols + 1};
-      float* p = dst + (size_t)(r * kPatchCols + q) * 8;
-      for (int k = 0; k < 4; ++k) {
-        p[2 * k] = m[corner[k]];
-        p[2 * k + 1] = c[corner[k]];
       }
     }
 }
@@ -347,13 +330,13 @@ void build_scan_layout(const HostLayers& h, std::vector<float>* site, std::vecto
   parallel_for((long long)kScanTables * L, threads, [&](long long lo, long long hi) {
     for (long long tl = lo; tl < hi; ++tl) {
       const int t = (int)(tl / L), k = (int)(tl % L);
-      pack_patches_mc(h.t[kSrc[t][0]].data() + (size_t)k * kCells,
+      pack_patches(h.t[kSrc[t][0]].data() + (size_t)k * kCells,
                       h.t[kSrc[t][1]].data() + (size_t)k * kCells,
                       site->data() + scan_layer_offset(t, k, L) * 4);
     }
   });
   chunk->assign(per_layer, 0.0f);
-  pack_patches_mc(h.t[kHomMean].data() + (size_t)(L - 1) * kCells,
+  pack_patches(h.t[kHomMean].data() + (size_t)(L - 1) * kCells,
                   h.t[kHomCv].data() + (size_t)(L - 1) * kCells, chunk->data());
 }
 

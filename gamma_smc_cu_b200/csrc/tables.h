@@ -36,7 +36,7 @@ struct HostLayers {
 };
 
 // Scan tables on the device: [direction][n_steps][hom, het][kPatches][8]
-// floats (patches of pack_patches_mc), so the hom and het patches of one
+// floats (patches of pack_patches), so the hom and het patches of one
 // layer are adjacent and a pair's
 // het bit selects between them with one multiply-add.  Offsets below are in
 // float4 units (two per patch).
@@ -60,10 +60,9 @@ int load_flow_field(const char* path, FlowField* ff, char* err, size_t err_len);
 void scaled_rates(double Ne, double mu, double rho, float* scaled_rho, float* scaled_mu);
 void build_layers(const FlowField& ff, int n_steps, float scaled_rho, float scaled_mu,
                   int threads, HostLayers* out);
-// 2450 patches of 8 floats from one [51 x 50] (m, c) layer: planar (m
-// corners, then c corners) or interleaved ((m, c) per corner, the scan's).
+// 2450 patches of 8 floats (four m corners, then four c corners) from one
+// [51 x 50] (m, c) layer.
 void pack_patches(const float* m, const float* c, float* dst);
-void pack_patches_mc(const float* m, const float* c, float* dst);
 void build_scan_layout(const HostLayers& h, std::vector<float>* site,
                        std::vector<float>* chunk, int threads);
 

@@ -14,7 +14,7 @@
 // Structure: the hom multi-step layers are independent per-cell chains (one
 // thread per grid cell, the flow field staged in shared memory); the
 // observed-site layers are independent per (layer, cell); a last kernel
-// packs the interleaved (m, c) patches of the scan layout.
+// packs the patches of the scan layout.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -155,7 +155,7 @@ __global__ void site_kernel(const double2* __restrict__ hom, const double* __res
 }
 
 // Scan layout: thread per (table t, layer k, patch p) writes the patch's
-// (m, c) corners interleaved (pack_patches_mc's layout).  Tables t < 4 are
+// four m corners, then its four c corners (pack_patches's layout).  Tables t < 4 are
 // the scan's fwd hom, fwd het, bwd hom, bwd het; the last kPatches threads
 // write the chunk table (hom layer L - 1).
 __global__ void pack_kernel(const float* __restrict__ out, const float* __restrict__ hom_f,
@@ -187,8 +187,8 @@ __global__ void pack_kernel(const float* __restrict__ out, const float* __restri
   const int corner[4] = {a, a + 1, a + kCols, a + kCols + 1};
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    dst[2 * i] = m[corner[i]];
-    dst[2 * i + 1] = c[corner[i]];
+    dst[i] = m[corner[i]];
+    dst[4 + i] = c[corner[i]];
   }
 }
 

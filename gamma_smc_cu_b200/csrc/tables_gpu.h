@@ -12,7 +12,7 @@ namespace gsmc {
 
 // Build the scan tables of L layers for (scaled_rho, scaled_mu) on the
 // current device in float64 and write them, rounded to float32, into the
-// device arrays site ([4][L][2450] interleaved patches) and chunk ([2450]
+// device arrays site ([4][L][2450] patches) and chunk ([2450]
 // patches of hom layer L - 1); the hom layers (float32) also go to the host
 // vectors.  0 on success, else -1 with *err set.
 int build_tables_gpu_f64(const FlowField& ff, int L, double scaled_rho, double scaled_mu,

@@ -55,13 +55,15 @@ __device__ __forceinline__ float floor_small(float x) {
 __device__ __forceinline__ Fetch patch_fetch(const float4* __restrict__ layer, float m, float c) {
   float fm = __fmul_rn(__fsub_rn(m, kMLo), kMInv);
   float fc = __fmul_rn(__fsub_rn(c, kCLo), kCInv);
+  // Lower-left corner: the reference clamps x to [0, last], truncates (x >= 0,
+  // so floor) and moves an index that lands on the last row/column down by
+  // one.  floor(max(0, min(x, last - 0.5))) is all of it at once -- equal to
+  // floor(min(clamp(x), last - 0.5)) for every x, NaN included -- and starts
+  // from the unclamped x, so the index does not wait for the weight's clamp.
+  const float rf = floor_small(fmaxf(0.0f, fminf(fm, (float)kPatchRows - 0.5f)));
+  const float qf = floor_small(fmaxf(0.0f, fminf(fc, (float)kPatchCols - 0.5f)));
   fm = fmaxf(0.0f, fminf(fm, (float)(kRows - 1)));
   fc = fmaxf(0.0f, fminf(fc, (float)(kCols - 1)));
-  // Lower-left corner: the reference truncates (fm >= 0, so floor) and moves
-  // an index that lands on the last row/column down by one.  floor(min(x,
-  // last - 0.5)) is both at once, and the weight stays x - corner.
-  const float rf = floor_small(fminf(fm, (float)kPatchRows - 0.5f));
-  const float qf = floor_small(fminf(fc, (float)kPatchCols - 0.5f));
   Fetch f;
   f.wm = __fsub_rn(fm, rf);
   f.wc = __fsub_rn(fc, qf);

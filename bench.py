@@ -966,6 +966,7 @@ def run_e2e(G, pos, pairs, core, flank, steps):
         ctx.close()
         return r, info, t_ctx
 
+    memory = "page-locked buffers reused across calls"
     prev = _core.set_result_memory("pinned")
     try:
         t0 = time.perf_counter()
@@ -979,10 +980,24 @@ def run_e2e(G, pos, pairs, core, flank, steps):
             times.append(time.perf_counter() - t0)
             ctx_s.append(t_ctx)
             del r
+    except MemoryError as e:   # the host could not page-lock the results
+        memory = f"pageable numpy arrays (page-locking failed: {e})"
+        times = None
     finally:
         _core.set_result_memory(prev)
         _lib.check(_lib.load().gsmc_host_cache_limit(0))        # give the memory back
         _lib.check(_lib.load().gsmc_host_cache_limit(256 << 30))
+    if times is None:
+        times, ctx_s = [], []
+        r, info0, _ = once()
+        first_s = 0.0
+        del r
+        for _ in range(max(1, steps)):
+            t0 = time.perf_counter()
+            r, info, t_ctx = once()
+            times.append(time.perf_counter() - t0)
+            ctx_s.append(t_ctx)
+            del r
     t0 = time.perf_counter()
     r, _, _ = once()
     pageable_s = time.perf_counter() - t0
@@ -991,7 +1006,7 @@ def run_e2e(G, pos, pairs, core, flank, steps):
     return {"value": P * sites / t, "unit": UNIT,
             "h2d_bytes_per_step": int(Gs.nbytes + ps.nbytes + 8 * P),
             "d2h_bytes_per_step": int(4 * sites * P), "seconds_per_step": t, "sites": sites,
-            "steps": len(times), "result_memory": "page-locked buffers reused across calls",
+            "steps": len(times), "result_memory": memory,
             "context_seconds_per_step": float(np.mean(ctx_s)),
             "first_call_seconds": first_s,
             "table_build_seconds_first_call": info0["build_seconds"],

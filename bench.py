@@ -336,6 +336,10 @@ def main():
     if args.workload == "chrom" and not args.no_full_posterior:
         full = run_full_posterior(G, pos, pairs, args.steps, args.warmup, dev)
 
+    tables64 = None
+    if args.workload == "chrom" and not args.no_full_posterior:
+        tables64 = run_tables_f64(G, pos)
+
     served = None
     if args.workload == "chrom" and not args.no_served:
         served = run_served(dev)
@@ -382,6 +386,7 @@ def main():
                          "bytes_per_pair_site": BYTES_MEAN_ONLY},
             "full_posterior": full,
             "summary": summary,
+            "tables_gpu_fp64": tables64,
             "batched": batched,
             "served": served,
             "stream_stress": stress,
@@ -735,6 +740,40 @@ def run_batched(ctx, G, dev, plain_jobs, jobs=None, workload=BATCH_WORKLOAD):
             "speedup_vs_plain_numpy_out": plain_s / batched_s,
             "speedup_vs_plain_pinned": plain_pinned_s / pinned_s,
             "max_rel_mean_vs_plain": max(err, err_pinned)}
+
+
+def run_tables_f64(G, pos, n_sites=50_000, n_pairs=4096):
+    """The optional float64 GPU table build against the bit-exact host float32
+    build: build seconds of each, and the posterior-mean deviation
+    (max relative) of the same calls through the two table sets -- the small
+    cohort's 780 pairs over its whole sequence, and 4,096 pairs of the
+    chromosome cohort's first 50,000 sites."""
+    from gamma_smc_cu_b200 import _core, synthetic
+    from gamma_smc_cu_b200.infer import _estimate_scaled_params
+    out = {}
+    Gs, ps = synthetic.cohort("small")
+    cases = [("small cohort, 780 pairs x 2,127 sites", Gs, ps, synthetic.all_pairs(Gs.shape[0])),
+             (f"chrom {n_sites}-site slice, {n_pairs} pairs",
+              np.ascontiguousarray(G[:, :n_sites]), np.ascontiguousarray(pos[:n_sites]),
+              synthetic.random_pairs(G.shape[0], n_pairs, 41))]
+    for name, Gc, pc, pairs in cases:
+        mu, rho = _estimate_scaled_params(Gc, pc, 1.25e-8, 1e-8, 1e4)
+        _core.free_cached_tables()
+        res = {}
+        for build in ("host_fp32", "gpu_fp64"):
+            ctx = _core.FlowContext(Gc, pc, 1e4, mu, rho, _core.DEFAULT_FLOW_FIELD, 0,
+                                    table_build=build)
+            secs = ctx.tables_info()["build_seconds"]
+            res[build] = (secs, ctx.run_fb(pairs, mean_only=True)["mean"])
+            ctx.close()
+        a, b = res["host_fp32"][1].astype(np.float64), res["gpu_fp64"][1].astype(np.float64)
+        rel = np.abs(b - a) / np.abs(a)
+        out[name] = {"build_seconds_host_fp32": res["host_fp32"][0],
+                     "build_seconds_gpu_fp64": res["gpu_fp64"][0],
+                     "mean_max_rel": float(rel.max()), "mean_median_rel": float(np.median(rel)),
+                     "within_1e-4": bool(rel.max() <= 1e-4)}
+    _core.free_cached_tables()
+    return out
 
 
 def run_summary(ctx, pairs, S, steps=2):

@@ -76,6 +76,8 @@ def parse():
     ap.add_argument("--case", default=None,
                     help="run one small profiling case instead of the benchmark")
     ap.add_argument("--repeat", type=int, default=1, help="repetitions of --case")
+    ap.add_argument("--watchdog", type=float, default=900.0,
+                    help="dump every thread's stack to stderr every this many seconds (0: off)")
     return ap.parse_args()
 
 
@@ -231,8 +233,21 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+_T0 = time.perf_counter()
+
+
+def log(msg):
+    """Progress of the run on stderr (the JSON line stays alone on stdout)."""
+    sys.stderr.write(f"[bench {time.perf_counter() - _T0:8.1f} s] {msg}\n")
+    sys.stderr.flush()
+
+
 def main():
     args = parse()
+    if args.watchdog > 0:
+        # if a leg stalls, the stacks of every thread show where
+        import faulthandler
+        faulthandler.dump_traceback_later(args.watchdog, repeat=True, file=sys.stderr)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -321,44 +336,55 @@ def main():
     torch.cuda.empty_cache()
     batched = None
     if args.workload == "chrom" and not args.no_batched:
+        log("batched")
         batched = run_batched(ctx, G, dev, args.plain_jobs)
     summary = None
     if args.workload == "chrom" and not args.no_summary:
+        log("summary")
         summary = run_summary(ctx, pairs, S)
     ctx.close()
     torch.cuda.empty_cache()
     if args.workload == "chrom" and not args.no_batched:
+        log("batched small cohort")
         batched["small_cohort"] = run_batched_small(dev)
     traffic = (TRAFFIC_PER_PAIR_SITE * psites.value / launches.value
                if launches.value and args.workload != "small" else None)
 
     full = None
     if args.workload == "chrom" and not args.no_full_posterior:
+        log("full posterior slice")
         full = run_full_posterior(G, pos, pairs, args.steps, args.warmup, dev)
 
     tables64 = None
     if args.workload == "chrom" and not args.no_full_posterior:
+        log("float64 tables")
         tables64 = run_tables_f64(G, pos)
 
     served = None
     if args.workload == "chrom" and not args.no_served:
+        log("served")
         served = run_served(dev)
     stress = None
     if args.workload == "chrom" and not args.no_stress and rank == 0:
+        log("stream stress")
         stress = run_stream_stress()
 
     e2e = None
     if not args.no_e2e:
+        log("e2e")
         e2e = run_e2e(G, pos, pairs, core, flank, args.e2e_steps)
     ref_gpu = None
     if args.workload == "chrom" and rank == 0 and not args.no_reference_gpu:
+        log("reference GPU build")
         ref_gpu = run_reference_gpu(G, pos, pairs, core, flank, mu, rho, cols, ours_cols,
                                     e2e, full)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        log("cpu baseline")
         cpu = cpu_baseline_sample(G, pos, pairs, core, flank, mu, rho)
     parity = None
     if rank == 0:
+        log("parity")
         parity = {"chrom": oracle_parity(G, pos, pairs[cols], mu, rho, core, flank,
                                          {"mean": ours_cols})}
         if full is not None:
@@ -567,6 +593,7 @@ def run_reference_gpu(G, pos, pairs, core, flank, mu, rho, cols, ours_cols, e2e,
     ctx = ref.FlowContext(Gs, ps, 1e4, mu, rho, DEFAULT_FLOW_FIELD, 0)
     r = ref.FlowContext.run_fb_blockwise(ctx, plist, int(core), int(flank), -1, 1, True, False)
     t = time.perf_counter() - t0
+    log(f"reference chromosome job {t:.1f} s")
     m = r["mean"]
     eq = bool(np.array_equal(np.ascontiguousarray(m[:, cols]).view(np.uint32),
                              np.ascontiguousarray(ours_cols[:sites]).view(np.uint32)))
@@ -581,6 +608,7 @@ def run_reference_gpu(G, pos, pairs, core, flank, mu, rho, cols, ours_cols, e2e,
         job["speedup_e2e_pageable"] = t / e2e["pageable_seconds"]
     # the reference's kernels alone, on 8,192 of the pairs (CUPTI activity
     # records of one run, taken separately from the wall-clock run above)
+    log("reference kernels (activity records)")
     sub = plist[:kernel_pairs]
     ctx = ref.FlowContext(Gs, ps, 1e4, mu, rho, DEFAULT_FLOW_FIELD, 0)
     r, ms = _cuda_kernel_ms(lambda: ref.FlowContext.run_fb_blockwise(
@@ -595,6 +623,7 @@ def run_reference_gpu(G, pos, pairs, core, flank, mu, rho, cols, ours_cols, e2e,
         n = 50_000
         Gs, ps = np.ascontiguousarray(G[:, :n]), np.ascontiguousarray(pos[:n])
         fmu, frho = full["mu"], full["rho"]
+        log("reference full-posterior slice")
         t0 = time.perf_counter()
         ctx = ref.FlowContext(Gs, ps, 1e4, fmu, frho, DEFAULT_FLOW_FIELD, 0)
         r = ref.FlowContext.run_fb(ctx, plist, True, True)
@@ -896,6 +925,7 @@ def run_served(dev, rates=(10, 100, 1000, 2000), seconds=2.0, burst=300):
                         "speedup": st["pair_sites_per_s"] / (ps / wall),
                         "served_batches": st.get("batches")}
         for rate in rates:
+            log(f"served rate {rate}/s")
             n = int(max(20, min(1000, rate * seconds)))
             reqs = synthetic.request_stream(pos, G.shape[0], n, rate, seed=6)
             st = _served_latency(srv, reqs)
@@ -1011,6 +1041,7 @@ def run_e2e(G, pos, pairs, core, flank, steps):
         t0 = time.perf_counter()
         r, info0, _ = once()   # builds the tables and the page-locked result buffer
         first_s = time.perf_counter() - t0
+        log(f"e2e first call (page-locked results) {first_s:.1f} s")
         del r
         times, ctx_s = [], []
         for _ in range(max(1, steps)):
@@ -1018,6 +1049,7 @@ def run_e2e(G, pos, pairs, core, flank, steps):
             r, info, t_ctx = once()
             times.append(time.perf_counter() - t0)
             ctx_s.append(t_ctx)
+            log(f"e2e step {times[-1]:.2f} s")
             del r
     except MemoryError as e:   # the host could not page-lock the results
         memory = f"pageable numpy arrays (page-locking failed: {e})"
@@ -1037,6 +1069,7 @@ def run_e2e(G, pos, pairs, core, flank, steps):
             times.append(time.perf_counter() - t0)
             ctx_s.append(t_ctx)
             del r
+    log("e2e pageable step")
     t0 = time.perf_counter()
     r, _, _ = once()
     pageable_s = time.perf_counter() - t0

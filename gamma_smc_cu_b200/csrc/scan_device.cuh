@@ -173,10 +173,20 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   const bool ci = (t.flags & kTaskCI) != 0, post = (t.flags & kTaskPosterior) != 0;
   constexpr bool summary = SUMMARY;
   const int j0 = threadIdx.x & (WIDTH - 1);
-  // Warps with no pair leave; lanes past the last pair of a partly filled warp
-  // walk along on pair (0, 0) with nothing stored (summary reductions need
-  // every lane of the warp).
-  if ((j0 & ~31) >= t.pair_count) return;
+  // Lanes past the last pair walk along on pair (0, 0) with nothing stored
+  // (summary reductions need every lane of the warp).  In a CTA-wide task
+  // every warp stays, even one with no pair: the task's warps meet at a
+  // barrier at each 32-site block (below).  A warp-wide task's empty warp
+  // leaves.
+  if (WIDTH != kThreads && (j0 & ~31) >= t.pair_count) return;
+  // CTA-wide tasks: the warps meet at the start of every 32-site block, so
+  // they walk within one block of each other and read the same table layers;
+  // the patches one warp brings into L1 are there when the others need them.
+  // (Chromosome job 210 -> 183 ms, full-posterior slice 42 -> 32 ms; without
+  // it the warps drift apart over a window and L1 hits stay near 51%.)
+  auto meet = [] {
+    if constexpr (WIDTH == kThreads) __syncthreads();
+  };
 
   const ulonglong2* gi[NP];
   const ulonglong2* gj[NP];
@@ -261,6 +271,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
     fp += kRow;
   }
   for (++s; s < cs;) {
+    meet();
     if ((s & 31) == 0) reload(s);
     for (const int e = min(cs, (s | 31) + 1); s < e; ++s) {
       const SiteCode nx2 = code[s + 2];
@@ -280,6 +291,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   };
   if (t.bl) record(t.bl, 1);
   while (s < ce) {
+    meet();
     if ((s & 31) == 0 && s != ps) reload(s);
     for (const int e = min(ce, (s | 31) + 1); s < e; ++s) {
       const SiteCode nx2 = code[s + 2];
@@ -327,6 +339,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   cur = code[s];
   nx = code[s - 1];
   while (s >= ce) {
+    meet();
     if ((s & 31) == 31 && s != pe - 1) reload(s);
     for (const int e = max(ce, s & ~31); s >= e; --s) {
       const SiteCode nx2 = code[s - 2];
@@ -351,6 +364,7 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   int64_t o = t.out_off + (int64_t)(ce - 1 - t.out_row0) * t.ldo + j0;
   s = ce - 1;
   while (s >= cs) {
+  meet();
   if ((s & 31) == 31 && s != pe - 1) reload(s);
   // unrolled by the ring depth so the ring rotation is register renaming
 #pragma unroll kFwdPrefetch

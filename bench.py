@@ -76,6 +76,7 @@ def parse():
     ap.add_argument("--case", default=None,
                     help="run one small profiling case instead of the benchmark")
     ap.add_argument("--repeat", type=int, default=1, help="repetitions of --case")
+    ap.add_argument("--reference-gpu-child", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--watchdog", type=float, default=900.0,
                     help="dump every thread's stack to stderr every this many seconds (0: off)")
     return ap.parse_args()
@@ -251,6 +252,9 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.reference_gpu_child:
+        reference_gpu_child(args.reference_gpu_child)
+        return
     if args.case:
         CASES[args.case](args.repeat)
         print(f"{args.case}: ok")
@@ -376,8 +380,7 @@ def main():
     ref_gpu = None
     if args.workload == "chrom" and rank == 0 and not args.no_reference_gpu:
         log("reference GPU build")
-        ref_gpu = run_reference_gpu(G, pos, pairs, core, flank, mu, rho, cols, ours_cols,
-                                    e2e, full)
+        ref_gpu = run_reference_gpu(G, pos, pairs, core, flank, mu, rho, full)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         log("cpu baseline")
@@ -566,92 +569,183 @@ def _scan_kernel_ms(ms):
     return sum(v for k, v in ms.items() if "gamma_smc_cached" in k or "precompute_xor" in k)
 
 
-def run_reference_gpu(G, pos, pairs, core, flank, mu, rho, cols, ours_cols, e2e, full,
-                      kernel_pairs=8192):
-    """Informational: the reference's own GPU build (its pybind11 _core from
-    the reference sources, compiled for sm_100a) on the same box and jobs,
-    through its public FlowContext API with host outputs, timed by wall clock
-    like ``e2e``: the chromosome job (FlowContext + run_fb_blockwise) and the
-    50k-site full-posterior slice (FlowContext + run_fb).  Reports seconds,
-    pair-sites/s, the speed-up of this build's same call, and whether the
-    sampled columns are bit-equal to this build's."""
-    import psutil
-    ref = _reference_core()
-    if ref is None:
-        return {"unavailable": "the reference _core was not built into oracle/_ref"}
+def reference_gpu_child(workdir):
+    """Child process of run_reference_gpu: runs the reference's own GPU build
+    on the saved inputs, writing each result to results.json as soon as it
+    exists (the parent may stop this process at its time limit)."""
     from gamma_smc_cu_b200._core import DEFAULT_FLOW_FIELD
-    out = {"build": "reference sources, nvcc 12.9 -gencode arch=compute_100a,code=sm_100a "
-                    "(its own CMake targets sm_80)"}
-    S, P = G.shape[1], len(pairs)
-    sites = S
-    avail = psutil.virtual_memory().available
-    if 4.0 * S * P > 0.45 * avail:
-        sites = int(0.45 * avail / (4.0 * P))
-    Gs, ps = np.ascontiguousarray(G[:, :sites]), np.ascontiguousarray(pos[:sites])
-    plist = [tuple(p) for p in pairs.tolist()]
+    ref = _reference_core()
+    d = np.load(os.path.join(workdir, "inputs.npz"))
+    with open(os.path.join(workdir, "params.json")) as f:
+        prm = json.load(f)
+    res = {}
+
+    def save():
+        with open(os.path.join(workdir, "results.json"), "w") as f:
+            json.dump(res, f)
+
+    G, pos = d["G"], d["pos"]
+    chrom = [tuple(p) for p in d["chrom_pairs"].tolist()]
+    core, flank = prm["core"], prm["flank"]
     t0 = time.perf_counter()
-    ctx = ref.FlowContext(Gs, ps, 1e4, mu, rho, DEFAULT_FLOW_FIELD, 0)
-    r = ref.FlowContext.run_fb_blockwise(ctx, plist, int(core), int(flank), -1, 1, True, False)
-    t = time.perf_counter() - t0
-    log(f"reference chromosome job {t:.1f} s")
-    m = r["mean"]
-    eq = bool(np.array_equal(np.ascontiguousarray(m[:, cols]).view(np.uint32),
-                             np.ascontiguousarray(ours_cols[:sites]).view(np.uint32)))
-    del r, m, ctx
-    job = {"workload": f"chrom: 356 haps x {sites} sites x {P} pairs, blockwise core {core} / "
-                       f"flank {flank}, mean_only, host outputs", "seconds": t,
-           "value": P * sites / t, "unit": UNIT, "sampled_columns_bit_equal": eq}
-    if e2e is not None and e2e.get("sites") == sites:
-        job["ours_e2e_seconds"] = e2e["seconds_per_step"]
-        job["speedup_e2e"] = t / e2e["seconds_per_step"]
-        job["ours_e2e_pageable_seconds"] = e2e["pageable_seconds"]
-        job["speedup_e2e_pageable"] = t / e2e["pageable_seconds"]
-    # the reference's kernels alone, on 8,192 of the pairs (CUPTI activity
-    # records of one run, taken separately from the wall-clock run above)
-    log("reference kernels (activity records)")
-    sub = plist[:kernel_pairs]
-    ctx = ref.FlowContext(Gs, ps, 1e4, mu, rho, DEFAULT_FLOW_FIELD, 0)
+    ctx = ref.FlowContext(G, pos, 1e4, prm["mu"], prm["rho"], DEFAULT_FLOW_FIELD, 0)
+    r = ref.FlowContext.run_fb_blockwise(ctx, chrom, core, flank, -1, 1, True, False)
+    res["chrom_seconds"] = time.perf_counter() - t0
+    np.save(os.path.join(workdir, "chrom_cols.npy"), np.ascontiguousarray(r["mean"][:, :64]))
+    del r
+    save()
     r, ms = _cuda_kernel_ms(lambda: ref.FlowContext.run_fb_blockwise(
-        ctx, sub, int(core), int(flank), -1, 1, True, False))
+        ctx, chrom, core, flank, -1, 1, True, False))
     del r, ctx
-    kms = _scan_kernel_ms(ms)
-    job["kernels"] = {"pairs": len(sub), "scan_kernel_ms": kms,
-                      "kernel_pair_sites_per_s": len(sub) * sites / (kms / 1e3) if kms else None,
-                      "by_kernel_ms": {k: v for k, v in sorted(ms.items(), key=lambda kv: -kv[1])[:6]}}
-    out["chrom"] = job
+    res["chrom_kernel_ms"] = _scan_kernel_ms(ms)
+    res["chrom_by_kernel_ms"] = {k: v for k, v in sorted(ms.items(), key=lambda kv: -kv[1])[:6]}
+    save()
+    n = prm["slice_sites"]
+    Gs, ps = np.ascontiguousarray(G[:, :n]), np.ascontiguousarray(pos[:n])
+    sl = [tuple(p) for p in d["slice_pairs"].tolist()]
+    t0 = time.perf_counter()
+    ctx = ref.FlowContext(Gs, ps, 1e4, prm["slice_mu"], prm["slice_rho"], DEFAULT_FLOW_FIELD, 0)
+    r = ref.FlowContext.run_fb(ctx, sl, True, True)
+    res["slice_seconds"] = time.perf_counter() - t0
+    np.savez(os.path.join(workdir, "slice_cols.npz"),
+             **{k: np.ascontiguousarray(r[k][:, :64])
+                for k in ("mean", "posterior_alpha", "posterior_beta")})
+    del r
+    save()
+    r, ms = _cuda_kernel_ms(lambda: ref.FlowContext.run_fb(ctx, sl, True, True))
+    del r, ctx
+    res["slice_kernel_ms"] = _scan_kernel_ms(ms)
+    save()
+
+
+def run_reference_gpu(G, pos, pairs, core, flank, mu, rho, full, chrom_pairs=1024,
+                      slice_pairs=2048, slice_sites=50_000, time_limit=240.0):
+    """Informational: the reference's own GPU build (its pybind11 _core from
+    the reference sources, compiled for sm_100a) on the same box, through its
+    public FlowContext API with host outputs, on bounded samples: the first
+    1,024 pairs of the chromosome job over all 400,000 sites (blockwise, the
+    same core and flank), and 2,048 pairs of the 50,000-site full-posterior
+    slice (run_fb with alpha/beta).  It runs in a child process stopped after
+    `time_limit` seconds (the full 63,190-pair job through it did not finish
+    within 23 minutes here); its kernel-only times come from CUDA activity
+    records of a second run.  This build's same calls run beside it, wall
+    clock and kernel events, and the first 64 pairs' columns are compared
+    bitwise."""
+    import shutil
+    import tempfile
+    from gamma_smc_cu_b200 import _core, _lib
+    from gamma_smc_cu_b200._core import DEFAULT_FLOW_FIELD
+    from gamma_smc_cu_b200.infer import _estimate_scaled_params
+    from oracle import oracle as O
+    if O.ref_core_path() is None:
+        return {"unavailable": "the reference _core was not built into oracle/_ref"}
+    S = G.shape[1]
+    cp = np.ascontiguousarray(pairs[:chrom_pairs])
+    sp = np.ascontiguousarray(pairs[:slice_pairs])
+    Gs, ps = np.ascontiguousarray(G[:, :slice_sites]), np.ascontiguousarray(pos[:slice_sites])
     if full is not None:
-        n = 50_000
-        Gs, ps = np.ascontiguousarray(G[:, :n]), np.ascontiguousarray(pos[:n])
-        fmu, frho = full["mu"], full["rho"]
-        log("reference full-posterior slice")
+        smu, srho = full["mu"], full["rho"]
+    else:
+        smu, srho = _estimate_scaled_params(Gs, ps, 1.25e-8, 1e-8, 1e4)
+    work = tempfile.mkdtemp(prefix="gsmc_refgpu_")
+    out = {"build": "reference sources, nvcc 12.9 -gencode arch=compute_100a,code=sm_100a "
+                    "(its own CMake targets sm_80)", "time_limit_s": time_limit}
+    try:
+        np.savez(os.path.join(work, "inputs.npz"), G=G, pos=pos, chrom_pairs=cp, slice_pairs=sp)
+        with open(os.path.join(work, "params.json"), "w") as f:
+            json.dump({"core": int(core), "flank": int(flank), "mu": mu, "rho": rho,
+                       "slice_sites": slice_sites, "slice_mu": smu, "slice_rho": srho}, f)
+        status = "finished"
+        try:
+            p = subprocess.run([sys.executable, os.path.abspath(__file__), "--reference-gpu-child",
+                                work], stdout=subprocess.DEVNULL, stderr=subprocess.PIPE,
+                               timeout=time_limit)
+            if p.returncode != 0:
+                status = f"exited {p.returncode}: {p.stderr.decode(errors='replace')[-300:]}"
+        except subprocess.TimeoutExpired:
+            status = f"stopped at the {time_limit:.0f} s limit"
+        out["status"] = status
+        rpath = os.path.join(work, "results.json")
+        res = json.load(open(rpath)) if os.path.exists(rpath) else {}
+
+        def ours(ctx, fn):
+            _lib.check(_lib.load().gsmc_ctx_timing_read(ctx.handle, None, None, None))
+            _lib.check(_lib.load().gsmc_ctx_timing(ctx.handle, 1))
+            r = fn()
+            kms = ctypes_double()
+            _lib.check(_lib.load().gsmc_ctx_timing_read(ctx.handle, kms.ref(), None, None))
+            _lib.check(_lib.load().gsmc_ctx_timing(ctx.handle, 0))
+            return r, kms.value
+
         t0 = time.perf_counter()
-        ctx = ref.FlowContext(Gs, ps, 1e4, fmu, frho, DEFAULT_FLOW_FIELD, 0)
-        r = ref.FlowContext.run_fb(ctx, plist, True, True)
-        t = time.perf_counter() - t0
-        want = {k: r[k][:, cols] for k in ("mean", "posterior_alpha", "posterior_beta")}
-        del r
-        r, ms = _cuda_kernel_ms(lambda: ref.FlowContext.run_fb(ctx, plist, True, True))
-        del r, ctx
-        kms = _scan_kernel_ms(ms)
-        from gamma_smc_cu_b200 import _core
-        t0 = time.perf_counter()
-        ctx = _core.FlowContext(Gs, ps, 1e4, fmu, frho, DEFAULT_FLOW_FIELD, 0)
-        o = ctx.run_fb(plist, mean_only=True, return_posterior=True)
+        ctx = _core.FlowContext(G, pos, 1e4, mu, rho, DEFAULT_FLOW_FIELD, 0)
+        r, kms = ours(ctx, lambda: ctx.run_fb_blockwise(
+            [tuple(x) for x in cp.tolist()], core_block_sites=int(core), flank_sites=int(flank),
+            pair_batch_size=len(cp), max_streams=1, mean_only=True))
         t_ours = time.perf_counter() - t0
+        job = {"workload": f"chrom: first {len(cp)} pairs x {S} sites, blockwise core {core} / "
+                           f"flank {flank}, mean_only, host outputs",
+               "ours_seconds": t_ours, "ours_kernel_ms": kms}
+        cpath = os.path.join(work, "chrom_cols.npy")
+        if os.path.exists(cpath):
+            job["sampled_columns_bit_equal"] = bool(np.array_equal(
+                np.load(cpath).view(np.uint32), np.ascontiguousarray(r["mean"][:, :64]).view(np.uint32)))
+        del r
         ctx.close()
-        eq = all(np.array_equal(np.ascontiguousarray(o[k][:, cols]).view(np.uint32),
-                                np.ascontiguousarray(w).view(np.uint32))
-                 for k, w in want.items())
-        del o
-        out["full_posterior"] = {
-            "workload": f"chrom 50k-site slice: {n} sites x {P} pairs, run_fb mean + alpha + "
-                        "beta, host outputs", "seconds": t, "value": P * n / t, "unit": UNIT,
-            "ours_seconds": t_ours, "speedup": t / t_ours, "sampled_columns_bit_equal": eq,
-            "scan_kernel_ms": kms,
-            "kernel_pair_sites_per_s": P * n / (kms / 1e3) if kms else None,
-            "ours_kernel_ms": full["roofline"]["kernel_ms_per_step"],
-            "kernel_speedup": kms / full["roofline"]["kernel_ms_per_step"] if kms else None}
+        if "chrom_seconds" in res:
+            job.update({"seconds": res["chrom_seconds"],
+                        "value": len(cp) * S / res["chrom_seconds"], "unit": UNIT,
+                        "speedup_wall": res["chrom_seconds"] / t_ours})
+        if res.get("chrom_kernel_ms"):
+            job.update({"kernel_ms": res["chrom_kernel_ms"],
+                        "kernel_pair_sites_per_s": len(cp) * S / (res["chrom_kernel_ms"] / 1e3),
+                        "kernel_speedup": res["chrom_kernel_ms"] / kms,
+                        "by_kernel_ms": res.get("chrom_by_kernel_ms")})
+        out["chrom"] = job
+        t0 = time.perf_counter()
+        ctx = _core.FlowContext(Gs, ps, 1e4, smu, srho, DEFAULT_FLOW_FIELD, 0)
+        r, kms = ours(ctx, lambda: ctx.run_fb([tuple(x) for x in sp.tolist()], mean_only=True,
+                                              return_posterior=True))
+        t_ours = time.perf_counter() - t0
+        sl = {"workload": f"chrom {slice_sites}-site slice: first {len(sp)} pairs, run_fb "
+                          "mean + alpha + beta, host outputs",
+              "ours_seconds": t_ours, "ours_kernel_ms": kms}
+        spath = os.path.join(work, "slice_cols.npz")
+        if os.path.exists(spath):
+            want = np.load(spath)
+            sl["sampled_columns_bit_equal"] = all(
+                np.array_equal(want[k].view(np.uint32),
+                               np.ascontiguousarray(r[k][:, :64]).view(np.uint32))
+                for k in ("mean", "posterior_alpha", "posterior_beta"))
+        del r
+        ctx.close()
+        if "slice_seconds" in res:
+            sl.update({"seconds": res["slice_seconds"],
+                       "value": len(sp) * slice_sites / res["slice_seconds"], "unit": UNIT,
+                       "speedup_wall": res["slice_seconds"] / t_ours})
+        if res.get("slice_kernel_ms"):
+            sl.update({"kernel_ms": res["slice_kernel_ms"],
+                       "kernel_speedup": res["slice_kernel_ms"] / kms})
+        out["full_posterior"] = sl
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
     return out
+
+
+class ctypes_double:
+    """A double out-parameter for the ctypes calls above."""
+
+    def __init__(self):
+        import ctypes
+        self._v = ctypes.c_double()
+        self._ref = ctypes.byref(self._v)
+
+    def ref(self):
+        return self._ref
+
+    @property
+    def value(self):
+        return float(self._v.value)
 
 
 def _max_rel(a, b):

@@ -573,7 +573,10 @@ def reference_gpu_child(workdir):
     """Child process of run_reference_gpu: runs the reference's own GPU build
     on the saved inputs, writing each result to results.json as soon as it
     exists (the parent may stop this process at its time limit)."""
+    import faulthandler
     from gamma_smc_cu_b200._core import DEFAULT_FLOW_FIELD
+    faulthandler.dump_traceback_later(60, repeat=True, file=sys.stderr)
+    log("child: loading the reference build")
     ref = _reference_core()
     d = np.load(os.path.join(workdir, "inputs.npz"))
     with open(os.path.join(workdir, "params.json")) as f:
@@ -587,10 +590,14 @@ def reference_gpu_child(workdir):
     G, pos = d["G"], d["pos"]
     chrom = [tuple(p) for p in d["chrom_pairs"].tolist()]
     core, flank = prm["core"], prm["flank"]
+    log(f"child: FlowContext {G.shape}")
     t0 = time.perf_counter()
     ctx = ref.FlowContext(G, pos, 1e4, prm["mu"], prm["rho"], DEFAULT_FLOW_FIELD, 0)
+    res["chrom_context_seconds"] = time.perf_counter() - t0
+    log(f"child: run_fb_blockwise {len(chrom)} pairs")
     r = ref.FlowContext.run_fb_blockwise(ctx, chrom, core, flank, -1, 1, True, False)
     res["chrom_seconds"] = time.perf_counter() - t0
+    log(f"child: done {res['chrom_seconds']:.1f} s")
     np.save(os.path.join(workdir, "chrom_cols.npy"), np.ascontiguousarray(r["mean"][:, :64]))
     del r
     save()
@@ -600,6 +607,7 @@ def reference_gpu_child(workdir):
     res["chrom_kernel_ms"] = _scan_kernel_ms(ms)
     res["chrom_by_kernel_ms"] = {k: v for k, v in sorted(ms.items(), key=lambda kv: -kv[1])[:6]}
     save()
+    log(f"child: kernels {res['chrom_kernel_ms']:.1f} ms")
     n = prm["slice_sites"]
     Gs, ps = np.ascontiguousarray(G[:, :n]), np.ascontiguousarray(pos[:n])
     sl = [tuple(p) for p in d["slice_pairs"].tolist()]
@@ -607,6 +615,7 @@ def reference_gpu_child(workdir):
     ctx = ref.FlowContext(Gs, ps, 1e4, prm["slice_mu"], prm["slice_rho"], DEFAULT_FLOW_FIELD, 0)
     r = ref.FlowContext.run_fb(ctx, sl, True, True)
     res["slice_seconds"] = time.perf_counter() - t0
+    log(f"child: slice {res['slice_seconds']:.1f} s")
     np.savez(os.path.join(workdir, "slice_cols.npz"),
              **{k: np.ascontiguousarray(r[k][:, :64])
                 for k in ("mean", "posterior_alpha", "posterior_beta")})
@@ -618,13 +627,13 @@ def reference_gpu_child(workdir):
     save()
 
 
-def run_reference_gpu(G, pos, pairs, core, flank, mu, rho, full, chrom_pairs=1024,
-                      slice_pairs=2048, slice_sites=50_000, time_limit=240.0):
+def run_reference_gpu(G, pos, pairs, core, flank, mu, rho, full, chrom_pairs=512,
+                      slice_pairs=1024, slice_sites=50_000, time_limit=240.0):
     """Informational: the reference's own GPU build (its pybind11 _core from
     the reference sources, compiled for sm_100a) on the same box, through its
     public FlowContext API with host outputs, on bounded samples: the first
-    1,024 pairs of the chromosome job over all 400,000 sites (blockwise, the
-    same core and flank), and 2,048 pairs of the 50,000-site full-posterior
+    512 pairs of the chromosome job over all 400,000 sites (blockwise, the
+    same core and flank), and 1,024 pairs of the 50,000-site full-posterior
     slice (run_fb with alpha/beta).  It runs in a child process stopped after
     `time_limit` seconds (the full 63,190-pair job through it did not finish
     within 23 minutes here); its kernel-only times come from CUDA activity
@@ -656,15 +665,21 @@ def run_reference_gpu(G, pos, pairs, core, flank, mu, rho, full, chrom_pairs=102
             json.dump({"core": int(core), "flank": int(flank), "mu": mu, "rho": rho,
                        "slice_sites": slice_sites, "slice_mu": smu, "slice_rho": srho}, f)
         status = "finished"
+        err = b""
         try:
             p = subprocess.run([sys.executable, os.path.abspath(__file__), "--reference-gpu-child",
                                 work], stdout=subprocess.DEVNULL, stderr=subprocess.PIPE,
                                timeout=time_limit)
+            err = p.stderr or b""
             if p.returncode != 0:
-                status = f"exited {p.returncode}: {p.stderr.decode(errors='replace')[-300:]}"
-        except subprocess.TimeoutExpired:
+                status = f"exited {p.returncode}"
+        except subprocess.TimeoutExpired as e:
             status = f"stopped at the {time_limit:.0f} s limit"
+            err = e.stderr or b""
         out["status"] = status
+        lines = [l for l in err.decode(errors="replace").splitlines() if l.strip()]
+        out["child_log"] = [l for l in lines if l.startswith("[bench")][-12:]
+        sys.stderr.write("\n".join(lines[-60:]) + "\n")
         rpath = os.path.join(work, "results.json")
         res = json.load(open(rpath)) if os.path.exists(rpath) else {}
 

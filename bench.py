@@ -51,6 +51,11 @@ BYTES_FULL_POSTERIOR = 12.25
 # sites x 63,190 pairs (`--case scan`): 16 B forward-state round trip + 4 B
 # output.
 TRAFFIC_PER_PAIR_SITE = 20.0
+# The same for the full posterior (mean + alpha + beta), from an ncu capture
+# of the 50,000-site slice's launch shape on 8,192 pairs (`--case
+# full_slice`): 11.44 GB over 4.1e8 core pair-sites -- 12 B of outputs, the
+# 16 B forward-state round trip, and the speculative chunks' burn-in reads.
+TRAFFIC_FULL_PER_PAIR_SITE = 28.0
 
 
 def parse():
@@ -508,7 +513,8 @@ def run_full_posterior(G, pos, pairs, steps, warmup, dev, n_sites=50_000):
             "gpu_launches": int(launches), "posterior_consistent": ok,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "peak_kind": kind,
-                         "bytes_per_pair_site": BYTES_FULL_POSTERIOR, "traffic": None,
+                         "bytes_per_pair_site": BYTES_FULL_POSTERIOR,
+                         "traffic": TRAFFIC_FULL_PER_PAIR_SITE * P * S,
                          "kernel_ms_per_step": kms}}
 
 
@@ -601,13 +607,7 @@ def reference_gpu_child(workdir):
     np.save(os.path.join(workdir, "chrom_cols.npy"), np.ascontiguousarray(r["mean"][:, :64]))
     del r
     save()
-    r, ms = _cuda_kernel_ms(lambda: ref.FlowContext.run_fb_blockwise(
-        ctx, chrom, core, flank, -1, 1, True, False))
-    del r, ctx
-    res["chrom_kernel_ms"] = _scan_kernel_ms(ms)
-    res["chrom_by_kernel_ms"] = {k: v for k, v in sorted(ms.items(), key=lambda kv: -kv[1])[:6]}
-    save()
-    log(f"child: kernels {res['chrom_kernel_ms']:.1f} ms")
+    del ctx
     n = prm["slice_sites"]
     Gs, ps = np.ascontiguousarray(G[:, :n]), np.ascontiguousarray(pos[:n])
     sl = [tuple(p) for p in d["slice_pairs"].tolist()]
@@ -625,15 +625,23 @@ def reference_gpu_child(workdir):
     del r, ctx
     res["slice_kernel_ms"] = _scan_kernel_ms(ms)
     save()
+    log("child: chromosome kernels")
+    ctx = ref.FlowContext(G, pos, 1e4, prm["mu"], prm["rho"], DEFAULT_FLOW_FIELD, 0)
+    r, ms = _cuda_kernel_ms(lambda: ref.FlowContext.run_fb_blockwise(
+        ctx, chrom, core, flank, -1, 1, True, False))
+    del r, ctx
+    res["chrom_kernel_ms"] = _scan_kernel_ms(ms)
+    res["chrom_by_kernel_ms"] = {k: v for k, v in sorted(ms.items(), key=lambda kv: -kv[1])[:6]}
+    save()
 
 
-def run_reference_gpu(G, pos, pairs, core, flank, mu, rho, full, chrom_pairs=512,
-                      slice_pairs=1024, slice_sites=50_000, time_limit=240.0):
+def run_reference_gpu(G, pos, pairs, core, flank, mu, rho, full, chrom_pairs=128,
+                      slice_pairs=512, slice_sites=50_000, time_limit=150.0):
     """Informational: the reference's own GPU build (its pybind11 _core from
     the reference sources, compiled for sm_100a) on the same box, through its
     public FlowContext API with host outputs, on bounded samples: the first
-    512 pairs of the chromosome job over all 400,000 sites (blockwise, the
-    same core and flank), and 1,024 pairs of the 50,000-site full-posterior
+    128 pairs of the chromosome job over all 400,000 sites (blockwise, the
+    same core and flank), and 512 pairs of the 50,000-site full-posterior
     slice (run_fb with alpha/beta).  It runs in a child process stopped after
     `time_limit` seconds (the full 63,190-pair job through it did not finish
     within 23 minutes here); its kernel-only times come from CUDA activity

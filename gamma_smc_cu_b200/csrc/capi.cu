@@ -326,6 +326,7 @@ struct gsmc_ctx {
   void* repair_pool = nullptr;            // forward-state slots of the repair launch
   size_t repair_pool_bytes = 0;
   bool speculate = true;                  // GSMC_SPECULATE=0 turns chunking off
+  double pool_fraction = 0.8;             // of free device memory for forward-state slots
   int spec_chunks_fixed = 0;              // GSMC_SPEC_CHUNKS: chunks per window, for measurements
   int64_t spec_flank = 2048;              // burn-in sites of a speculative chunk
   int64_t spec_launches = 0;              // launches that ran speculative chunks
@@ -409,7 +410,7 @@ int resident_ctas(ScanShape shape) {
 }
 
 int spec_chunks(const gsmc_ctx* ctx, int64_t tasks, int64_t resident_tiles, int64_t core_len,
-                int flags);
+                int flags, double row_bytes = 0.0, double slot_budget = 0.0);
 double launch_cost(int64_t n, int64_t r, double steps);
 double chunk_steps(int64_t core_len, int K, int64_t b);
 int64_t max_core(const std::vector<Block>& blocks);
@@ -582,15 +583,17 @@ struct SpecLaunch {
 
 // Estimated duration, in pair-steps of one tile, of a persistent launch of n
 // equal tasks of `steps` pair-steps each on r resident tiles: full waves of r
-// tasks, and a partial last wave that runs faster (fewer CTAs share the SMs)
-// but not in proportion to its size -- modelled as max(fraction, 0.8) of a
-// full wave (on the 50,000-site full-posterior slice, 63,190 pairs: 988
-// tasks on 1,184 tiles took 42 ms, 1,482 took 50 ms, 1,235 took 55 ms).
+// tasks plus a partial wave of fraction f.  A partial wave runs faster than
+// its share of the GPU (fewer CTAs share the SMs) and, after full waves,
+// overlaps their uneven ends; fitted on the 50,000-site full-posterior slice
+// (63,190 pairs, 1,184 resident tiles, 2 to 8 chunks): alone it costs
+// 0.3 + 0.64 f of a full wave, after full waves 0.26 + 0.37 f.
 double launch_cost(int64_t n, int64_t r, double steps) {
   if (n <= 0 || r <= 0) return 0.0;
   const int64_t full = n / r;
-  const double frac = (double)(n % r) / (double)r;
-  return steps * ((double)full + (frac > 0.0 ? std::max(frac, 0.8) : 0.0));
+  const double f = (double)(n % r) / (double)r;
+  const double part = f <= 0.0 ? 0.0 : (full == 0 ? 0.3 + 0.64 * f : 0.26 + 0.37 * f);
+  return steps * ((double)full + part);
 }
 
 // Longest task (pair-steps per pair) of a core of core_len sites cut into K
@@ -604,19 +607,26 @@ double chunk_steps(int64_t core_len, int K, int64_t b) {
 // Chunks per window for a launch of `tasks` tasks on `resident_tiles`
 // tiles: none when the tasks fill the GPU twice; otherwise the K (chunks of
 // at least two burn-ins) that minimises launch_cost -- balancing the
-// burn-in steps each extra chunk adds against filling the last wave.
+// burn-in steps each extra chunk adds against filling the last wave.  With
+// a slot budget, a tile's forward-state slot holds ceil(core / K) rows of
+// `row_bytes`, and only the tiles whose slots fit the budget run at once.
 int spec_chunks(const gsmc_ctx* ctx, int64_t tasks, int64_t resident_tiles, int64_t core_len,
-                int flags) {
+                int flags, double row_bytes, double slot_budget) {
   if (!ctx->speculate || (flags & kTaskSummary) || tasks <= 0) return 1;
   if (ctx->spec_chunks_fixed > 0)
     return (int)std::max<int64_t>(1, std::min<int64_t>(ctx->spec_chunks_fixed, core_len / 64));
   if (tasks >= 2 * resident_tiles) return 1;
   const int64_t b = ctx->spec_flank;
   const int k_max = (int)std::max<int64_t>(1, std::min<int64_t>(1024, core_len / (2 * b)));
+  auto tiles_for = [&](int K) {
+    if (slot_budget <= 0.0 || row_bytes <= 0.0) return resident_tiles;
+    const double fit = slot_budget / ((double)ceil_div(core_len, K) * row_bytes);
+    return std::max<int64_t>(1, std::min<int64_t>(resident_tiles, (int64_t)fit));
+  };
   int best = 1;
-  double best_cost = launch_cost(tasks, resident_tiles, chunk_steps(core_len, 1, b));
+  double best_cost = launch_cost(tasks, tiles_for(1), chunk_steps(core_len, 1, b));
   for (int K = 2; K <= k_max; ++K) {
-    const double c = launch_cost(tasks * K, resident_tiles, chunk_steps(core_len, K, b));
+    const double c = launch_cost(tasks * K, tiles_for(K), chunk_steps(core_len, K, b));
     if (c < best_cost * 0.999) {
       best = K;
       best_cost = c;
@@ -726,10 +736,12 @@ int run_direct(gsmc_ctx* ctx, const int32_t* d_pi, const int32_t* d_pj, int64_t 
   const int tile = scan_tile_pairs(ctx->shape);
   const int64_t resident_tiles = (int64_t)resident_ctas(ctx->shape) * scan_tiles_per_cta(ctx->shape);
   const int64_t plain_tasks = (int64_t)blocks.size() * ceil_div(P, tile);
+  const size_t budget = (size_t)(ctx->pool_fraction * (double)free_device_bytes()) + ctx->pool_bytes;
   std::vector<int> K(blocks.size());
   int64_t n_bnd = 0;
   for (size_t i = 0; i < blocks.size(); ++i) {
-    K[i] = spec_chunks(ctx, plain_tasks, resident_tiles, blocks[i].ce - blocks[i].cs, flags);
+    K[i] = spec_chunks(ctx, plain_tasks, resident_tiles, blocks[i].ce - blocks[i].cs, flags,
+                       (double)tile * sizeof(float2), (double)budget);
     n_bnd += K[i] - 1;
   }
   int rc = spec_reserve(ctx, n_bnd, P);
@@ -743,7 +755,6 @@ int run_direct(gsmc_ctx* ctx, const int32_t* d_pi, const int32_t* d_pj, int64_t 
                           2.0f * ctx->ne, ctx->spec_rec, &sl, &tasks);
   int64_t slot_rows = 0;
   for (const Task& t : tasks) slot_rows = std::max<int64_t>(slot_rows, t.ce - t.cs);
-  const size_t budget = (size_t)(0.8 * (double)free_device_bytes()) + ctx->pool_bytes;
   const int want = (int)std::min<int64_t>(resident_ctas(ctx->shape),
                                           ceil_div((int64_t)tasks.size(), scan_tiles_per_cta(ctx->shape)));
   int grid = 0;
@@ -821,7 +832,8 @@ int run_to_host(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int6
   int64_t slot_rows = 0, max_k = 1;
   for (size_t i = 0; i < blocks.size(); ++i) {
     const int64_t len = blocks[i].ce - blocks[i].cs;
-    K[i] = spec_chunks(ctx, group * ceil_div(chunk, ptile), resident_tiles, len, flags);
+    K[i] = spec_chunks(ctx, group * ceil_div(chunk, ptile), resident_tiles, len, flags,
+                       (double)ptile * sizeof(float2), (double)pool_budget);
     slot_rows = std::max(slot_rows, ceil_div(len, K[i]));
     max_k = std::max<int64_t>(max_k, K[i]);
   }
@@ -970,6 +982,8 @@ int gsmc_ctx_create_ex(const uint8_t* G, int64_t n_haps, int64_t n_sites, const 
     ctx->spec_flank = std::max<int64_t>(1, std::atoll(env));
   if (const char* env = std::getenv("GSMC_SPEC_CHUNKS"))
     ctx->spec_chunks_fixed = std::max(0, std::atoi(env));
+  if (const char* env = std::getenv("GSMC_POOL_FRACTION"))
+    ctx->pool_fraction = std::min(0.97, std::max(0.1, std::atof(env)));
   if (const char* env = std::getenv("GSMC_SCAN_WIDTH")) {
     const int v = std::atoi(env);
     if (v == 32 || v == 128) ctx->shape.width = v;

@@ -327,6 +327,7 @@ struct gsmc_ctx {
   size_t repair_pool_bytes = 0;
   bool speculate = true;                  // GSMC_SPECULATE=0 turns chunking off
   double pool_fraction = 0.8;             // of free device memory for forward-state slots
+  int64_t spec_max_chunk = 16384;         // longest chunk core when a window is cut (0: no cap)
   int spec_chunks_fixed = 0;              // GSMC_SPEC_CHUNKS: chunks per window, for measurements
   int64_t spec_flank = 2048;              // burn-in sites of a speculative chunk
   int64_t spec_launches = 0;              // launches that ran speculative chunks
@@ -623,16 +624,24 @@ int spec_chunks(const gsmc_ctx* ctx, int64_t tasks, int64_t resident_tiles, int6
     const double fit = slot_budget / ((double)ceil_div(core_len, K) * row_bytes);
     return std::max<int64_t>(1, std::min<int64_t>(resident_tiles, (int64_t)fit));
   };
-  int best = 1;
-  double best_cost = launch_cost(tasks, tiles_for(1), chunk_steps(core_len, 1, b));
-  for (int K = 2; K <= k_max; ++K) {
-    const double c = launch_cost(tasks * K, tiles_for(K), chunk_steps(core_len, K, b));
-    if (c < best_cost * 0.999) {
-      best = K;
-      best_cost = c;
-    }
+  // Once a window is cut, its chunks are kept short: with the same waves,
+  // chunks of 15-17k sites ran faster than 33k-site ones (the per-site
+  // summary's 23,600-pair batches over 400,000 sites: 0.25 s at 27 chunks,
+  // 0.32 s at 12), as did the slice's 12.5k-site chunks.
+  const int k_min = ctx->spec_max_chunk > 0
+                        ? (int)std::min<int64_t>(k_max, ceil_div(core_len, ctx->spec_max_chunk))
+                        : 1;
+  // The model ranks close plans only to about 5%: take the fewest chunks
+  // (fewest burn-ins and boundaries to verify) within 5% of the cheapest.
+  std::vector<double> cost(k_max + 1, 1e300);
+  double lowest = 1e300;
+  for (int K = k_min; K <= k_max; ++K) {
+    cost[K] = launch_cost(tasks * K, tiles_for(K), chunk_steps(core_len, K, b));
+    lowest = std::min(lowest, cost[K]);
   }
-  return best;
+  for (int K = k_min; K <= k_max; ++K)
+    if (cost[K] <= 1.05 * lowest) return K;
+  return k_min;
 }
 
 // Append the tasks of window b for the n pairs at (pi, pj): whole, or in K
@@ -982,6 +991,8 @@ int gsmc_ctx_create_ex(const uint8_t* G, int64_t n_haps, int64_t n_sites, const 
     ctx->spec_flank = std::max<int64_t>(1, std::atoll(env));
   if (const char* env = std::getenv("GSMC_SPEC_CHUNKS"))
     ctx->spec_chunks_fixed = std::max(0, std::atoi(env));
+  if (const char* env = std::getenv("GSMC_SPEC_MAX_CHUNK"))
+    ctx->spec_max_chunk = std::max<int64_t>(0, std::atoll(env));
   if (const char* env = std::getenv("GSMC_POOL_FRACTION"))
     ctx->pool_fraction = std::min(0.97, std::max(0.1, std::atof(env)));
   if (const char* env = std::getenv("GSMC_SCAN_WIDTH")) {

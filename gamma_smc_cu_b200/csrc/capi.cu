@@ -598,11 +598,28 @@ double launch_cost(int64_t n, int64_t r, double steps) {
 }
 
 // Longest task (pair-steps per pair) of a core of core_len sites cut into K
-// chunks with burn-in b: each interior boundary adds b forward steps to the
-// right chunk and b backward steps to the left one.
+// chunks with burn-in b, cut as chunk_cuts does (no window flanks): each
+// interior boundary adds b forward steps to the right chunk and b backward
+// steps to the left one, and the cuts share those steps out evenly.
 double chunk_steps(int64_t core_len, int K, int64_t b) {
-  const double c = (double)ceil_div(core_len, K);
-  return 2.0 * c + (K >= 3 ? 2.0 * b : K == 2 ? (double)b : 0.0);
+  if (K <= 1) return 2.0 * (double)core_len;
+  return (2.0 * (double)core_len + 2.0 * (K - 1) * (double)b) / K;
+}
+
+// Cut points of window b's core into K speculative chunks of equal
+// pair-steps (chunk_cuts in windows.h).
+std::vector<int64_t> chunk_cuts(const Block& b, int K, int64_t flank) {
+  std::vector<int64_t> c(std::max(K, 1) + 1);
+  gsmc::chunk_cuts(b.ps, b.cs, b.ce, b.pe, std::max(K, 1), flank, c.data());
+  return c;
+}
+
+// Longest chunk core of window b cut into K chunks.
+int64_t longest_chunk(const Block& b, int K, int64_t flank) {
+  const std::vector<int64_t> c = chunk_cuts(b, K, flank);
+  int64_t m = 0;
+  for (int k = 0; k < K; ++k) m = std::max(m, c[k + 1] - c[k]);
+  return m;
 }
 
 // Chunks per window for a launch of `tasks` tasks on `resident_tiles`
@@ -657,8 +674,9 @@ void add_spec_window_tasks(const Block& b, int K, int64_t flank, const int32_t* 
   }
   const int64_t len = b.ce - b.cs;
   const int64_t bnd0 = sl->n_bnd;
+  const std::vector<int64_t> cut = chunk_cuts(b, K, flank);
   for (int k = 0; k < K; ++k) {
-    const int64_t c0 = b.cs + len * k / K, c1 = b.cs + len * (k + 1) / K;
+    const int64_t c0 = cut[k], c1 = cut[k + 1];
     const Block cb{c0, c1, k == 0 ? b.ps : std::max(b.ps, c0 - flank),
                    k == K - 1 ? b.pe : std::min(b.pe, c1 + flank)};
     const size_t first = tasks->size();
@@ -843,7 +861,7 @@ int run_to_host(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int6
     const int64_t len = blocks[i].ce - blocks[i].cs;
     K[i] = spec_chunks(ctx, group * ceil_div(chunk, ptile), resident_tiles, len, flags,
                        (double)ptile * sizeof(float2), (double)pool_budget);
-    slot_rows = std::max(slot_rows, ceil_div(len, K[i]));
+    slot_rows = std::max(slot_rows, K[i] > 1 ? longest_chunk(blocks[i], K[i], ctx->spec_flank) : len);
     max_k = std::max<int64_t>(max_k, K[i]);
   }
   // CTAs one launch can keep busy: its (chunk, pair tile) tasks, at most

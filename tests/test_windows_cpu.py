@@ -80,3 +80,81 @@ def test_zero_sites_has_no_window(driver):
     out = subprocess.run([driver], input="0 5 3\n", capture_output=True, text=True,
                          check=True).stdout
     assert out.strip() == "0"
+
+
+CUTS_DRIVER = r"""
+#include <cstdio>
+#include "windows.h"
+int main() {
+  long long ps, cs, ce, pe, flank;
+  int K;
+  while (std::scanf("%lld %lld %lld %lld %d %lld", &ps, &cs, &ce, &pe, &K, &flank) == 6) {
+    long long cut[1100];
+    int64_t c64[1100];
+    gsmc::chunk_cuts(ps, cs, ce, pe, K, flank, c64);
+    for (int k = 0; k <= K; ++k) cut[k] = c64[k];
+    for (int k = 0; k <= K; ++k) std::printf("%lld ", cut[k]);
+    std::printf("\n");
+  }
+  return 0;
+}
+"""
+
+
+@pytest.fixture(scope="module")
+def cuts_driver(tmp_path_factory):
+    d = tmp_path_factory.mktemp("cuts")
+    src = d / "cuts.cpp"
+    src.write_text(CUTS_DRIVER)
+    exe = d / "cuts"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", CSRC, str(src), "-o", str(exe)], check=True)
+    return str(exe)
+
+
+def _steps(ps, cs, ce, pe, flank, cut):
+    K = len(cut) - 1
+    out = []
+    for k in range(K):
+        pre = cs - ps if k == 0 else flank
+        post = pe - ce if k == K - 1 else flank
+        out.append(2 * (cut[k + 1] - cut[k]) + pre + post)
+    return out
+
+
+def test_chunk_cuts_balance_pair_steps(cuts_driver):
+    """Speculative chunk cuts cover the core exactly, in order, and give every
+    chunk the same forward + backward steps (to rounding): a chunk at a
+    sequence end, which runs no burn-in on that side, gets the steps as
+    extra core.  Windows with flanks on both sides as long as the burn-in
+    are cut into equal lengths."""
+    cases = [
+        (0, 0, 50_000, 50_000, 4, 2048),           # one window over a whole slice
+        (0, 0, 50_000, 50_000, 9, 2048),
+        (0, 0, 32_768, 34_816, 3, 2048),            # first window of a chromosome
+        (30_720, 32_768, 65_536, 67_584, 5, 2048),  # interior window
+        (393_216 - 2048, 393_216, 400_000, 400_000, 2, 2048),
+        (0, 0, 400_000, 400_000, 25, 2048),
+        (0, 0, 10, 10, 3, 2048),                    # too short: equal lengths
+        (0, 0, 1 << 40, 1 << 40, 1000, 2048),
+    ]
+    inp = "".join(f"{a} {b} {c} {d} {K} {f}\n" for a, b, c, d, K, f in cases)
+    out = subprocess.run([cuts_driver], input=inp, capture_output=True, text=True,
+                         check=True).stdout.strip().splitlines()
+    assert len(out) == len(cases)
+    for (ps, cs, ce, pe, K, flank), line in zip(cases, out):
+        cut = [int(x) for x in line.split()]
+        assert len(cut) == K + 1
+        assert cut[0] == cs and cut[-1] == ce
+        assert all(b > a for a, b in zip(cut, cut[1:])) or ce - cs < K
+        lens = [b - a for a, b in zip(cut, cut[1:])]
+        if min(lens) < flank:
+            # fallback: the equal-length cuts
+            assert cut == [cs + (ce - cs) * k // K for k in range(K + 1)]
+            continue
+        st = _steps(ps, cs, ce, pe, flank, cut)
+        assert max(st) - min(st) <= 4, (ps, cs, ce, pe, K, st)
+        if cs - ps == flank and pe - ce == flank:
+            assert max(lens) - min(lens) <= 2
+    # the slice: edge chunks take the missing burn-in as core
+    cut = [int(x) for x in out[0].split()]
+    assert [b - a for a, b in zip(cut, cut[1:])] == [13012, 11988, 11988, 13012]

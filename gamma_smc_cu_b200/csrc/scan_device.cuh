@@ -52,31 +52,55 @@ __device__ __forceinline__ float floor_small(float x) {
   return __fsub_rn(__fadd_rd(x, 8388608.0f), 8388608.0f);
 }
 
-__device__ __forceinline__ Fetch patch_fetch(const float4* __restrict__ layer, float m, float c) {
-  float fm = __fmul_rn(__fsub_rn(m, kMLo), kMInv);
-  float fc = __fmul_rn(__fsub_rn(c, kCLo), kCInv);
+// Address of patch 0 of `layer` minus 0x4B000000 patches (unsigned, wraps):
+// adding (0x4B000000 + index) patches gives the patch.
+__device__ __forceinline__ uint64_t biased(const float4* layer) {
+  return reinterpret_cast<uint64_t>(layer) - ((uint64_t)0x4B000000u << 5);
+}
+
+// Lookup of (m, c) in the hom (het = 0) or het (het = 1) half of the layer
+// whose biased base is layer_bias.
+__device__ __forceinline__ Fetch patch_fetch(uint64_t layer_bias, int het, float m, float c) {
+  const float fm = __fmul_rn(__fsub_rn(m, kMLo), kMInv);
+  const float fc = __fmul_rn(__fsub_rn(c, kCLo), kCInv);
   // Lower-left corner: the reference clamps x to [0, last], truncates (x >= 0,
   // so floor) and moves an index that lands on the last row/column down by
   // one.  floor(max(0, min(x, last - 0.5))) is all of it at once -- equal to
   // floor(min(clamp(x), last - 0.5)) for every x, NaN included -- and starts
   // from the unclamped x, so the index does not wait for the weight's clamp.
-  const float rf = floor_small(fmaxf(0.0f, fminf(fm, (float)kPatchRows - 0.5f)));
-  const float qf = floor_small(fmaxf(0.0f, fminf(fc, (float)kPatchCols - 0.5f)));
-  fm = fmaxf(0.0f, fminf(fm, (float)(kRows - 1)));
-  fc = fmaxf(0.0f, fminf(fc, (float)(kCols - 1)));
+  // The floor is (y +rd 2^23) - 2^23 (floor_small); the biased sums are kept
+  // for the patch index below.
+  const float rb = __fadd_rd(fmaxf(0.0f, fminf(fm, (float)kPatchRows - 0.5f)), 8388608.0f);
+  const float qb = __fadd_rd(fmaxf(0.0f, fminf(fc, (float)kPatchCols - 0.5f)), 8388608.0f);
+  const float rf = __fsub_rn(rb, 8388608.0f);
+  const float qf = __fsub_rn(qb, 8388608.0f);
   Fetch f;
-  f.wm = __fsub_rn(fm, rf);
-  f.wc = __fsub_rn(fc, qf);
-  // rf * 49 + qf is an exact integer below 2450; adding 2^23 places it in the
-  // low mantissa bits, so the patch index needs no conversion instruction.
-  const int idx = __float_as_int(__fadd_rn(__fmaf_rn(rf, (float)kPatchCols, qf), 8388608.0f)) -
-                  0x4B000000;
+  // Weight clamp(x, 0, last) - floor as one saturated subtract: for x < 0 the
+  // floor is 0 and both give +0 (x is never -0: it is (v - lo) * step, and
+  // v - lo rounds an exact zero to +0); inside [0, last] the clamp does
+  // nothing and x - floor lies in [0, 1]; above last the reference's weight is
+  // last - (last - 1) = 1 and x - (last - 1) > 1 saturates to 1.  The two
+  // differ only for x = NaN (the reference's clamp gives last, .sat gives 0),
+  // and x is never NaN: every table value is clamped to the grid when the
+  // tables are built (NaN included), so the states -- 0 at the start of a
+  // window, then bilinear blends of table values -- stay finite.
+  f.wm = __saturatef(__fsub_rn(fm, rf));
+  f.wc = __saturatef(__fsub_rn(fc, qf));
+  // rf * 49 + qf is an exact integer below 2450, so rf * 49 + (qf + 2^23) is
+  // exact too and sits in the low mantissa bits: the patch index needs no
+  // conversion instruction.
+  const uint32_t bits = (uint32_t)__float_as_int(__fmaf_rn(rf, (float)kPatchCols, qb));
+  const int idx = (int)(bits - 0x4B000000u);
+  // The het half of a layer starts kPatches patches after the hom half, so
+  // the half is one more integer add on the biased index, and the address is
+  // one wide multiply-add from the biased layer base.
+  const uint32_t key = bits + (uint32_t)(het * kPatches);
   // One 256-bit read-only load of the 32-byte patch: m corners (r,q) (r,q+1)
   // (r+1,q) (r+1,q+1), then the c corners.  Patches are 32-byte aligned:
   // table bases come from cudaMalloc and every layer, hom/het half and patch
   // offset is a multiple of 32 bytes.
   f.idx = idx;
-  const float4* p = layer + kPatchF4 * idx;
+  const float4* p = reinterpret_cast<const float4*>(layer_bias + ((uint64_t)key << 5));
   asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
       : "=f"(f.a.x), "=f"(f.a.y), "=f"(f.a.z), "=f"(f.a.w), "=f"(f.b.x), "=f"(f.b.y),
         "=f"(f.b.z), "=f"(f.b.w)
@@ -94,7 +118,7 @@ __device__ __forceinline__ void patch_interp(const Fetch& f, float& m, float& c)
 
 __device__ __forceinline__ void patch_lookup(const float4* __restrict__ layer, float& m,
                                              float& c) {
-  const Fetch f = patch_fetch(layer, m, c);
+  const Fetch f = patch_fetch(biased(layer), 0, m, c);
   patch_interp(f, m, c);
 }
 
@@ -244,12 +268,13 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
       }
     }
     const float4* layer = fwd_tab + sc.layer;
+    const uint64_t lb = biased(layer);
     Fetch f[NP];
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
       const int het = (int)(x[k] & 1u);
       x[k] >>= 1;
-      f[k] = patch_fetch(layer + het * kHetF4, m[k], c[k]);
+      f[k] = patch_fetch(lb, het, m[k], c[k]);
       prefetch_patch(fwd_tab + next_layer + (int)(x[k] & 1u) * kHetF4 + kPatchF4 * f[k].idx);
     }
 #pragma unroll
@@ -316,12 +341,12 @@ __device__ __forceinline__ void scan_task(const ScanArgs& a, const Task& t, floa
   // Backward step at site s: the het/hom site table first, then any full
   // 1000-bp chunks.
   auto bwd_fetch = [&](int s, SiteCode sc, int next_layer, Fetch* f) {
-    const float4* layer = bwd_tab + sc.layer;
+    const uint64_t lb = biased(bwd_tab + sc.layer);
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
       const int het = (int)(x[k] >> 31);
       x[k] <<= 1;
-      f[k] = patch_fetch(layer + het * kHetF4, m[k], c[k]);
+      f[k] = patch_fetch(lb, het, m[k], c[k]);
       prefetch_patch(bwd_tab + next_layer + (int)(x[k] >> 31) * kHetF4 + kPatchF4 * f[k].idx);
     }
   };

@@ -47,6 +47,30 @@ def _free_device_bytes(device):
     return torch.cuda.mem_get_info(device)[0]
 
 
+def _prewarm(device, streams, device_bytes, pinned_bytes):
+    """Fill the allocator caches a batch draws on, before serving starts.
+
+    A batch's device buffers come from torch's caching allocator on its slot's
+    stream, and cached blocks are kept per stream, so a slot's first batch of
+    a new size calls cudaMalloc -- and, with little free memory, releases the
+    cache with cudaFree, which waits for the device: milliseconds inside the
+    scheduler loop.  One block of ``device_bytes`` per stream, freed at once,
+    stays cached for that stream and is split for later batches.  Pinned
+    staging of pair indices (torch's caching host allocator, power-of-two
+    size classes) is warmed up to ``pinned_bytes`` the same way."""
+    import torch
+    for st in streams:
+        with torch.cuda.stream(st):
+            t = torch.empty(max(int(device_bytes), 1), dtype=torch.uint8, device=device)
+        del t
+    n = 4096
+    while n <= max(int(pinned_bytes), 4096):
+        t = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+        del t
+        n *= 2
+    torch.cuda.synchronize(device)
+
+
 def _new_arena(nbytes):
     return PinnedArena(nbytes)
 
@@ -183,6 +207,10 @@ class TmrcaServer:
         self.max_batch_requests = int(max_batch_requests)
         self.max_batch_pair_sites = float(max_batch_pair_sites)
         self.arena = _new_arena(pinned_bytes) if pinned_bytes else None
+        # a batch's outputs fit the largest arena block (or wait for one)
+        _prewarm(self.device, [sl.stream for sl in self.slots],
+                 min(self.hbm_budget, int(pinned_bytes) if pinned_bytes else 1 << 28),
+                 min(8 * self.max_tasks * 128, 8 << 20))
         self.poll_interval = float(poll_interval)
         self._pending = collections.deque()
         self._cv = threading.Condition()
@@ -197,6 +225,7 @@ class TmrcaServer:
         # (what the loop was doing), and the cyclic garbage collector's pauses
         # while serving (they stop the scheduler thread too).
         self._stalls = []          # (ms, what)
+        self._admit_step = ""
         self._gc_pauses = []       # (generation, ms)
         self._gc_t0 = None
         if freeze_gc:
@@ -418,15 +447,24 @@ class TmrcaServer:
         now = time.perf_counter()
         for r in take:
             r.t_admit = now
+        # the slowest step of this admission names a loop stall (_loop)
+        steps = [now]
         try:
             layout = Layout([r.job for r in take])
+            steps.append(time.perf_counter())
             host = self.arena.alloc(layout.out_floats * BYTES_PER_FLOAT) if self.arena else None
             if host is None:
                 host = _pinned_floats(layout.out_floats)
                 with self._cv:
                     self.counters["outside_arena"] += 1
+            steps.append(time.perf_counter())
             batch = DeviceBatch(layout, self.device)
+            steps.append(time.perf_counter())
             batch.launch(slot.executor, slot.stream, host=host)
+            steps.append(time.perf_counter())
+            names = ("layout", "host", "batch", "launch")
+            d = [b - a for a, b in zip(steps, steps[1:])]
+            self._admit_step = names[d.index(max(d))]
         except Exception as e:  # a launch failure fails the batch's queries
             with self._cv:
                 self._in_use -= nbytes
@@ -452,8 +490,9 @@ class TmrcaServer:
                 if slot.batch is None and self._pending:
                     free = True
                     t0 = time.perf_counter()
+                    self._admit_step = "queue"
                     busy |= self._admit(slot)
-                    self._note_stall(t0, "admit")
+                    self._note_stall(t0, "admit:" + self._admit_step)
             if self._pending and not free:
                 self.counters["wait_executor"] += 1
             with self._cv:

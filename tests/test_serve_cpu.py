@@ -120,6 +120,7 @@ def server_factory(monkeypatch):
         monkeypatch.setattr(serve, "_free_device_bytes", lambda d: 1 << 30)
         monkeypatch.setattr(serve, "_bind_thread", lambda d: None)
         monkeypatch.setattr(serve, "_new_arena", NumpyArena)
+        monkeypatch.setattr(serve, "_prewarm", lambda *a: None)
         monkeypatch.setattr(serve, "_pinned_floats", lambda n: np.zeros(max(n, 1), np.float32))
         positions = np.arange(500, dtype=np.float64) * 10.0
         s = serve.TmrcaServer(FakeCtx(), positions=positions, **kw)

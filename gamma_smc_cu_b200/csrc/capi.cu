@@ -50,12 +50,21 @@ std::vector<std::pair<void*, uint64_t>> g_host_free;
 uint64_t g_host_cached = 0;
 uint64_t g_host_cache_cap = uint64_t(256) << 30;
 
-void trim_host_cache_locked() {
+// Take cached blocks out until the cache is within its cap; the caller frees
+// them with free_host_blocks after releasing g_host_mu (unpinning a large
+// block takes seconds, and other threads' allocations must not wait on it).
+std::vector<std::pair<void*, uint64_t>> trim_host_cache_locked() {
+  std::vector<std::pair<void*, uint64_t>> out;
   while (g_host_cached > g_host_cache_cap && !g_host_free.empty()) {
-    cudaFreeHost(g_host_free.front().first);
+    out.push_back(g_host_free.front());
     g_host_cached -= g_host_free.front().second;
     g_host_free.erase(g_host_free.begin());
   }
+  return out;
+}
+
+void free_host_blocks(const std::vector<std::pair<void*, uint64_t>>& blocks) {
+  for (const auto& kv : blocks) cudaFreeHost(kv.first);
 }
 
 // mbarrier polls the uncached kernels wait for their flow-field copy.
@@ -1934,56 +1943,76 @@ int gsmc_host_alloc(uint64_t bytes, void** ptr) {
   if (!ptr) return fail(GSMC_E_INVALID, "null output pointer");
   *ptr = nullptr;
   if (bytes == 0) bytes = 1;
-  std::lock_guard<std::mutex> lock(g_host_mu);
-  // the smallest cached block that fits without wasting more than half of it
-  auto best = g_host_free.end();
-  for (auto it = g_host_free.begin(); it != g_host_free.end(); ++it)
-    if (it->second >= bytes && it->second / 2 <= bytes &&
-        (best == g_host_free.end() || it->second < best->second))
-      best = it;
-  if (best != g_host_free.end()) {
-    *ptr = best->first;
-    g_host_used[best->first] = best->second;
-    g_host_cached -= best->second;
-    g_host_free.erase(best);
-    return GSMC_OK;
+  {
+    std::lock_guard<std::mutex> lock(g_host_mu);
+    // the smallest cached block that fits without wasting more than half of it
+    auto best = g_host_free.end();
+    for (auto it = g_host_free.begin(); it != g_host_free.end(); ++it)
+      if (it->second >= bytes && it->second / 2 <= bytes &&
+          (best == g_host_free.end() || it->second < best->second))
+        best = it;
+    if (best != g_host_free.end()) {
+      *ptr = best->first;
+      g_host_used[best->first] = best->second;
+      g_host_cached -= best->second;
+      g_host_free.erase(best);
+      return GSMC_OK;
+    }
   }
+  // Page-locking runs outside the lock: it takes seconds for tens of GB.
   void* p = nullptr;
   cudaError_t e = cudaHostAlloc(&p, bytes, cudaHostAllocPortable);
-  if (e != cudaSuccess && !g_host_free.empty()) {
+  if (e != cudaSuccess) {
     // release the cache and try once more
     cudaGetLastError();
-    for (auto& kv : g_host_free) cudaFreeHost(kv.first);
-    g_host_free.clear();
-    g_host_cached = 0;
-    e = cudaHostAlloc(&p, bytes, cudaHostAllocPortable);
+    std::vector<std::pair<void*, uint64_t>> drop;
+    {
+      std::lock_guard<std::mutex> lock(g_host_mu);
+      drop.swap(g_host_free);
+      g_host_cached = 0;
+    }
+    if (!drop.empty()) {
+      free_host_blocks(drop);
+      e = cudaHostAlloc(&p, bytes, cudaHostAllocPortable);
+    }
   }
   if (e != cudaSuccess) {
     cudaGetLastError();
     return fail(GSMC_E_NOMEM, "CUDA error: %s (page-locked host buffer of %llu bytes)",
                 cudaGetErrorString(e), (unsigned long long)bytes);
   }
-  g_host_used[p] = bytes;
+  {
+    std::lock_guard<std::mutex> lock(g_host_mu);
+    g_host_used[p] = bytes;
+  }
   *ptr = p;
   return GSMC_OK;
 }
 
 int gsmc_host_free(void* ptr) {
   if (!ptr) return GSMC_OK;
-  std::lock_guard<std::mutex> lock(g_host_mu);
-  auto it = g_host_used.find(ptr);
-  if (it == g_host_used.end()) return fail(GSMC_E_INVALID, "not a gsmc_host_alloc buffer");
-  g_host_free.emplace_back(it->first, it->second);
-  g_host_cached += it->second;
-  g_host_used.erase(it);
-  trim_host_cache_locked();
+  std::vector<std::pair<void*, uint64_t>> drop;
+  {
+    std::lock_guard<std::mutex> lock(g_host_mu);
+    auto it = g_host_used.find(ptr);
+    if (it == g_host_used.end()) return fail(GSMC_E_INVALID, "not a gsmc_host_alloc buffer");
+    g_host_free.emplace_back(it->first, it->second);
+    g_host_cached += it->second;
+    g_host_used.erase(it);
+    drop = trim_host_cache_locked();
+  }
+  free_host_blocks(drop);
   return GSMC_OK;
 }
 
 int gsmc_host_cache_limit(uint64_t max_cached_bytes) {
-  std::lock_guard<std::mutex> lock(g_host_mu);
-  g_host_cache_cap = max_cached_bytes;
-  trim_host_cache_locked();
+  std::vector<std::pair<void*, uint64_t>> drop;
+  {
+    std::lock_guard<std::mutex> lock(g_host_mu);
+    g_host_cache_cap = max_cached_bytes;
+    drop = trim_host_cache_locked();
+  }
+  free_host_blocks(drop);
   return GSMC_OK;
 }
 

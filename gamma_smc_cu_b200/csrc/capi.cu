@@ -337,6 +337,7 @@ struct gsmc_ctx {
   bool speculate = true;                  // GSMC_SPECULATE=0 turns chunking off
   double pool_fraction = 0.8;             // of free device memory for forward-state slots
   int64_t spec_max_chunk = 16384;         // longest chunk core when a window is cut (0: no cap)
+  double core_weight = 1.0;               // cost of a core site in burn-in sites (chunk cuts)
   int spec_chunks_fixed = 0;              // GSMC_SPEC_CHUNKS: chunks per window, for measurements
   int64_t spec_flank = 2048;              // burn-in sites of a speculative chunk
   int64_t spec_launches = 0;              // launches that ran speculative chunks
@@ -422,7 +423,7 @@ int resident_ctas(ScanShape shape) {
 int spec_chunks(const gsmc_ctx* ctx, int64_t tasks, int64_t resident_tiles, int64_t core_len,
                 int flags, double row_bytes = 0.0, double slot_budget = 0.0);
 double launch_cost(int64_t n, int64_t r, double steps);
-double chunk_steps(int64_t core_len, int K, int64_t b);
+double chunk_steps(int64_t core_len, int K, int64_t b, double w);
 int64_t max_core(const std::vector<Block>& blocks);
 
 // Launch shape of a call over P pairs x `blocks`: two pairs per thread (two
@@ -439,7 +440,7 @@ void pick_shape(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int 
     const int64_t tasks = (int64_t)blocks.size() * ceil_div(P, scan_tile_pairs(sh));
     const int64_t tiles = (int64_t)resident_ctas(sh) * scan_tiles_per_cta(sh);
     const int K = spec_chunks(ctx, tasks, tiles, core, flags);
-    return per_step * launch_cost(tasks * K, tiles, chunk_steps(core, K, ctx->spec_flank));
+    return per_step * launch_cost(tasks * K, tiles, chunk_steps(core, K, ctx->spec_flank, ctx->core_weight));
   };
   const int64_t tasks2 = (int64_t)blocks.size() * ceil_div(P, scan_tile_pairs(two));
   const bool use_two = tasks2 >= 2 * resident_ctas(two) || cost(two, 1.45) <= cost(one, 1.0);
@@ -606,26 +607,27 @@ double launch_cost(int64_t n, int64_t r, double steps) {
   return steps * ((double)full + part);
 }
 
-// Longest task (pair-steps per pair) of a core of core_len sites cut into K
-// chunks with burn-in b, cut as chunk_cuts does (no window flanks): each
-// interior boundary adds b forward steps to the right chunk and b backward
-// steps to the left one, and the cuts share those steps out evenly.
-double chunk_steps(int64_t core_len, int K, int64_t b) {
-  if (K <= 1) return 2.0 * (double)core_len;
-  return (2.0 * (double)core_len + 2.0 * (K - 1) * (double)b) / K;
+// Longest task (burn-in-step units per pair) of a core of core_len sites cut
+// into K chunks with burn-in b, cut as chunk_cuts does (no window flanks):
+// each interior boundary adds b forward steps to the right chunk and b
+// backward steps to the left one, a core site costs w, and the cuts share the
+// cost out evenly.
+double chunk_steps(int64_t core_len, int K, int64_t b, double w) {
+  if (K <= 1) return 2.0 * w * (double)core_len;
+  return (2.0 * w * (double)core_len + 2.0 * (K - 1) * (double)b) / K;
 }
 
-// Cut points of window b's core into K speculative chunks of equal
-// pair-steps (chunk_cuts in windows.h).
-std::vector<int64_t> chunk_cuts(const Block& b, int K, int64_t flank) {
+// Cut points of window b's core into K speculative chunks of equal cost
+// (chunk_cuts in windows.h).
+std::vector<int64_t> chunk_cuts(const Block& b, int K, int64_t flank, double w) {
   std::vector<int64_t> c(std::max(K, 1) + 1);
-  gsmc::chunk_cuts(b.ps, b.cs, b.ce, b.pe, std::max(K, 1), flank, c.data());
+  gsmc::chunk_cuts(b.ps, b.cs, b.ce, b.pe, std::max(K, 1), flank, w, c.data());
   return c;
 }
 
 // Longest chunk core of window b cut into K chunks.
-int64_t longest_chunk(const Block& b, int K, int64_t flank) {
-  const std::vector<int64_t> c = chunk_cuts(b, K, flank);
+int64_t longest_chunk(const Block& b, int K, int64_t flank, double w) {
+  const std::vector<int64_t> c = chunk_cuts(b, K, flank, w);
   int64_t m = 0;
   for (int k = 0; k < K; ++k) m = std::max(m, c[k + 1] - c[k]);
   return m;
@@ -664,7 +666,7 @@ int spec_chunks(const gsmc_ctx* ctx, int64_t tasks, int64_t resident_tiles, int6
   std::vector<double> cost(k_max + 1, 1e300);
   double lowest = 1e300;
   for (int K = k_min; K <= k_max; ++K) {
-    cost[K] = launch_cost(tasks * K, tiles_for(K), chunk_steps(core_len, K, b));
+    cost[K] = launch_cost(tasks * K, tiles_for(K), chunk_steps(core_len, K, b, ctx->core_weight));
     lowest = std::min(lowest, cost[K]);
   }
   for (int K = k_min; K <= k_max; ++K)
@@ -675,7 +677,7 @@ int spec_chunks(const gsmc_ctx* ctx, int64_t tasks, int64_t resident_tiles, int6
 // Append the tasks of window b for the n pairs at (pi, pj): whole, or in K
 // speculative chunks whose boundary records start at record `sl->n_bnd` of
 // `rec` (already sized).
-void add_spec_window_tasks(const Block& b, int K, int64_t flank, const int32_t* pi,
+void add_spec_window_tasks(const Block& b, int K, int64_t flank, double core_weight, const int32_t* pi,
                            const int32_t* pj, int64_t n, int tile, const WindowOut& wo,
                            int64_t col, int flags, float unscale, float2* rec, SpecLaunch* sl,
                            std::vector<Task>* tasks) {
@@ -685,7 +687,7 @@ void add_spec_window_tasks(const Block& b, int K, int64_t flank, const int32_t* 
   }
   const int64_t len = b.ce - b.cs;
   const int64_t bnd0 = sl->n_bnd;
-  const std::vector<int64_t> cut = chunk_cuts(b, K, flank);
+  const std::vector<int64_t> cut = chunk_cuts(b, K, flank, core_weight);
   for (int k = 0; k < K; ++k) {
     const int64_t c0 = cut[k], c1 = cut[k + 1];
     const Block cb{c0, c1, k == 0 ? b.ps : std::max(b.ps, c0 - flank),
@@ -788,7 +790,7 @@ int run_direct(gsmc_ctx* ctx, const int32_t* d_pi, const int32_t* d_pj, int64_t 
   SpecLaunch sl;
   WindowOut wo{{out[0], out[1], out[2], out[3], out[4]}, 0, ld, 0};
   for (size_t i = 0; i < blocks.size(); ++i)
-    add_spec_window_tasks(blocks[i], K[i], ctx->spec_flank, d_pi, d_pj, P, tile, wo, col0,
+    add_spec_window_tasks(blocks[i], K[i], ctx->spec_flank, ctx->core_weight, d_pi, d_pj, P, tile, wo, col0,
                           task_flags(flags),
                           2.0f * ctx->ne, ctx->spec_rec, &sl, &tasks);
   int64_t slot_rows = 0;
@@ -872,7 +874,7 @@ int run_to_host(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int6
     const int64_t len = blocks[i].ce - blocks[i].cs;
     K[i] = spec_chunks(ctx, group * ceil_div(chunk, ptile), resident_tiles, len, flags,
                        (double)ptile * sizeof(float2), (double)pool_budget);
-    slot_rows = std::max(slot_rows, K[i] > 1 ? longest_chunk(blocks[i], K[i], ctx->spec_flank) : len);
+    slot_rows = std::max(slot_rows, K[i] > 1 ? longest_chunk(blocks[i], K[i], ctx->spec_flank, ctx->core_weight) : len);
     max_k = std::max<int64_t>(max_k, K[i]);
   }
   // CTAs one launch can keep busy: its (chunk, pair tile) tasks, at most
@@ -913,7 +915,7 @@ int run_to_host(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int6
         wo.off = i * core * n;
         wo.ldo = n;
         wo.row0 = b.cs;
-        add_spec_window_tasks(b, K[g0 + i], ctx->spec_flank, d_pi + off, d_pj + off, n, ptile, wo, 0,
+        add_spec_window_tasks(b, K[g0 + i], ctx->spec_flank, ctx->core_weight, d_pi + off, d_pj + off, n, ptile, wo, 0,
                               task_flags(flags), 2.0f * ctx->ne, ctx->spec_rec, &sl, &tasks);
       }
       rc = launch_tasks(ctx, tasks, h, slot_rows, grid, ctx->stream);
@@ -1020,6 +1022,8 @@ int gsmc_ctx_create_ex(const uint8_t* G, int64_t n_haps, int64_t n_sites, const 
     ctx->spec_flank = std::max<int64_t>(1, std::atoll(env));
   if (const char* env = std::getenv("GSMC_SPEC_CHUNKS"))
     ctx->spec_chunks_fixed = std::max(0, std::atoi(env));
+  if (const char* env = std::getenv("GSMC_CORE_WEIGHT"))
+    ctx->core_weight = std::min(8.0, std::max(0.25, std::atof(env)));
   if (const char* env = std::getenv("GSMC_SPEC_MAX_CHUNK"))
     ctx->spec_max_chunk = std::max<int64_t>(0, std::atoll(env));
   if (const char* env = std::getenv("GSMC_POOL_FRACTION"))

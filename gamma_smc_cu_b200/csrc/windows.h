@@ -60,28 +60,31 @@ GSMC_HD WindowBounds window_bounds(int64_t w, int64_t n_sites, int64_t core_bloc
 }
 
 // Cut points cut[0] = cs < cut[1] < ... < cut[K] = ce of the core of window
-// [ps, pe) into K >= 1 speculative chunks of equal pair-steps (host only).
-// Chunk k runs forward from cut[k] - pre_k to cut[k+1] and backward from
+// [ps, pe) into K >= 1 speculative chunks of equal cost (host only).  Chunk
+// k runs forward from cut[k] - pre_k to cut[k+1] and backward from
 // cut[k+1] + post_k to cut[k], where pre_0 = cs - ps (the window's own left
 // flank), pre_k = flank otherwise, post_(K-1) = pe - ce and post_k = flank
-// otherwise, so it takes 2 len_k + pre_k + post_k steps.  Equal steps T give
-// len_k = (T - pre_k - post_k) / 2: a chunk at an end of the sequence, where
-// the window has no flank, takes the steps of the burn-in it does not run as
-// extra core.  Equal lengths when a chunk would come out shorter than one
-// flank (or than one site).
+// otherwise.  A core site costs core_weight burn-in sites (its forward step
+// also stores the state, its backward step reads it back and combines), so
+// chunk k costs 2 w len_k + pre_k + post_k.  Equal cost T gives
+// len_k = (T - pre_k - post_k) / (2 w): a chunk at an end of the sequence,
+// where the window has no flank, takes the cost of the burn-in it does not
+// run as extra core.  Equal lengths when a chunk would come out shorter than
+// one flank (or than one site).
 inline void chunk_cuts(int64_t ps, int64_t cs, int64_t ce, int64_t pe, int K, int64_t flank,
-                       int64_t* cut) {
+                       double core_weight, int64_t* cut) {
   const int64_t len = ce - cs;
   for (int k = 0; k <= K; ++k) cut[k] = cs + len * k / K;
   if (K <= 1) return;
+  const double w = core_weight > 0.0 ? core_weight : 1.0;
   const double e0 = (double)(cs - ps), e1 = (double)(pe - ce), f = (double)flank;
-  const double T = (2.0 * (double)len + e0 + e1 + 2.0 * (K - 1) * f) / K;
+  const double T = (2.0 * w * (double)len + e0 + e1 + 2.0 * (K - 1) * f) / K;
   const int64_t min_len = flank > 1 ? flank : 1;
   double acc = 0.0;
   int64_t prev = cs;
   for (int k = 0; k < K; ++k) {
     const double pre = k == 0 ? e0 : f, post = k == K - 1 ? e1 : f;
-    acc += 0.5 * (T - pre - post);
+    acc += (T - pre - post) / (2.0 * w);
     const int64_t next = k == K - 1 ? ce : cs + (int64_t)std::llround(acc);
     if (next - prev < min_len) {
       for (int j = 0; j <= K; ++j) cut[j] = cs + len * j / K;

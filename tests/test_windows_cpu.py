@@ -88,10 +88,11 @@ CUTS_DRIVER = r"""
 int main() {
   long long ps, cs, ce, pe, flank;
   int K;
-  while (std::scanf("%lld %lld %lld %lld %d %lld", &ps, &cs, &ce, &pe, &K, &flank) == 6) {
+  double w;
+  while (std::scanf("%lld %lld %lld %lld %d %lld %lf", &ps, &cs, &ce, &pe, &K, &flank, &w) == 7) {
     long long cut[1100];
     int64_t c64[1100];
-    gsmc::chunk_cuts(ps, cs, ce, pe, K, flank, c64);
+    gsmc::chunk_cuts(ps, cs, ce, pe, K, flank, w, c64);
     for (int k = 0; k <= K; ++k) cut[k] = c64[k];
     for (int k = 0; k <= K; ++k) std::printf("%lld ", cut[k]);
     std::printf("\n");
@@ -111,13 +112,13 @@ def cuts_driver(tmp_path_factory):
     return str(exe)
 
 
-def _steps(ps, cs, ce, pe, flank, cut):
+def _steps(ps, cs, ce, pe, flank, cut, w=1.0):
     K = len(cut) - 1
     out = []
     for k in range(K):
         pre = cs - ps if k == 0 else flank
         post = pe - ce if k == K - 1 else flank
-        out.append(2 * (cut[k + 1] - cut[k]) + pre + post)
+        out.append(2 * w * (cut[k + 1] - cut[k]) + pre + post)
     return out
 
 
@@ -137,11 +138,13 @@ def test_chunk_cuts_balance_pair_steps(cuts_driver):
         (0, 0, 10, 10, 3, 2048),                    # too short: equal lengths
         (0, 0, 1 << 40, 1 << 40, 1000, 2048),
     ]
-    inp = "".join(f"{a} {b} {c} {d} {K} {f}\n" for a, b, c, d, K, f in cases)
+    cases += [case[:6] + (1.5,) for case in cases[:6]]
+    cases = [c if len(c) == 7 else c + (1.0,) for c in cases]
+    inp = "".join(f"{a} {b} {c} {d} {K} {f} {w}\n" for a, b, c, d, K, f, w in cases)
     out = subprocess.run([cuts_driver], input=inp, capture_output=True, text=True,
                          check=True).stdout.strip().splitlines()
     assert len(out) == len(cases)
-    for (ps, cs, ce, pe, K, flank), line in zip(cases, out):
+    for (ps, cs, ce, pe, K, flank, w), line in zip(cases, out):
         cut = [int(x) for x in line.split()]
         assert len(cut) == K + 1
         assert cut[0] == cs and cut[-1] == ce
@@ -151,10 +154,15 @@ def test_chunk_cuts_balance_pair_steps(cuts_driver):
             # fallback: the equal-length cuts
             assert cut == [cs + (ce - cs) * k // K for k in range(K + 1)]
             continue
-        st = _steps(ps, cs, ce, pe, flank, cut)
-        assert max(st) - min(st) <= 4, (ps, cs, ce, pe, K, st)
+        st = _steps(ps, cs, ce, pe, flank, cut, w)
+        assert max(st) - min(st) <= 4 * w, (ps, cs, ce, pe, K, w, st)
         if cs - ps == flank and pe - ce == flank:
             assert max(lens) - min(lens) <= 2
-    # the slice: edge chunks take the missing burn-in as core
+    # the slice: an edge chunk runs one burn-in fewer and takes its cost as
+    # core, flank / (2 w) sites more (a core site is walked forward and
+    # backward, w burn-in sites each): 1,024 at w = 1, 683 at w = 1.5
     cut = [int(x) for x in out[0].split()]
     assert [b - a for a, b in zip(cut, cut[1:])] == [13012, 11988, 11988, 13012]
+    cut = [int(x) for x in out[8].split()]
+    lens = [b - a for a, b in zip(cut, cut[1:])]
+    assert lens[0] == lens[3] and lens[1] == lens[2] and abs(lens[0] - lens[1] - 683) <= 2

@@ -337,7 +337,14 @@ struct gsmc_ctx {
   bool speculate = true;                  // GSMC_SPECULATE=0 turns chunking off
   double pool_fraction = 0.8;             // of free device memory for forward-state slots
   int64_t spec_max_chunk = 16384;         // longest chunk core when a window is cut (0: no cap)
-  double core_weight = 1.0;               // cost of a core site in burn-in sites (chunk cuts)
+  // Cost of a core site in burn-in sites when chunk cuts are balanced: its
+  // forward step also stores the state, its backward step reads it back and
+  // combines.  2 measured best of 1-2 (8,192 pairs x 50,000 sites, 12 chunks:
+  // 7.25 -> 6.70 ms; all 63,190 pairs, 4 chunks: 31.46 -> 31.17 ms).  The
+  // chunk-count model keeps counting plain pair-steps: its wave coefficients
+  // were fitted that way, and weighting there moved the slice to 9 chunks
+  // (33 ms against 31).
+  double core_weight = 2.0;
   int spec_chunks_fixed = 0;              // GSMC_SPEC_CHUNKS: chunks per window, for measurements
   int64_t spec_flank = 2048;              // burn-in sites of a speculative chunk
   int64_t spec_launches = 0;              // launches that ran speculative chunks
@@ -440,7 +447,7 @@ void pick_shape(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int 
     const int64_t tasks = (int64_t)blocks.size() * ceil_div(P, scan_tile_pairs(sh));
     const int64_t tiles = (int64_t)resident_ctas(sh) * scan_tiles_per_cta(sh);
     const int K = spec_chunks(ctx, tasks, tiles, core, flags);
-    return per_step * launch_cost(tasks * K, tiles, chunk_steps(core, K, ctx->spec_flank, ctx->core_weight));
+    return per_step * launch_cost(tasks * K, tiles, chunk_steps(core, K, ctx->spec_flank, 1.0));
   };
   const int64_t tasks2 = (int64_t)blocks.size() * ceil_div(P, scan_tile_pairs(two));
   const bool use_two = tasks2 >= 2 * resident_ctas(two) || cost(two, 1.45) <= cost(one, 1.0);
@@ -666,7 +673,7 @@ int spec_chunks(const gsmc_ctx* ctx, int64_t tasks, int64_t resident_tiles, int6
   std::vector<double> cost(k_max + 1, 1e300);
   double lowest = 1e300;
   for (int K = k_min; K <= k_max; ++K) {
-    cost[K] = launch_cost(tasks * K, tiles_for(K), chunk_steps(core_len, K, b, ctx->core_weight));
+    cost[K] = launch_cost(tasks * K, tiles_for(K), chunk_steps(core_len, K, b, 1.0));
     lowest = std::min(lowest, cost[K]);
   }
   for (int K = k_min; K <= k_max; ++K)

@@ -641,7 +641,8 @@ int64_t longest_chunk(const Block& b, int K, int64_t flank, double w) {
 }
 
 // Chunks per window for a launch of `tasks` tasks on `resident_tiles`
-// tiles: none when the tasks fill the GPU twice; otherwise the K (chunks of
+// tiles: when the tasks fill the GPU twice, only as many as keep chunks
+// within the chunk cap; otherwise the K (chunks of
 // at least two burn-ins) that minimises launch_cost -- balancing the
 // burn-in steps each extra chunk adds against filling the last wave.  With
 // a slot budget, a tile's forward-state slot holds ceil(core / K) rows of
@@ -651,9 +652,17 @@ int spec_chunks(const gsmc_ctx* ctx, int64_t tasks, int64_t resident_tiles, int6
   if (!ctx->speculate || (flags & kTaskSummary) || tasks <= 0) return 1;
   if (ctx->spec_chunks_fixed > 0)
     return (int)std::max<int64_t>(1, std::min<int64_t>(ctx->spec_chunks_fixed, core_len / 64));
-  if (tasks >= 2 * resident_tiles) return 1;
   const int64_t b = ctx->spec_flank;
   const int k_max = (int)std::max<int64_t>(1, std::min<int64_t>(1024, core_len / (2 * b)));
+  // Launches that fill the GPU twice over need no chunks to fill it, but
+  // windows longer than the chunk cap are still cut to it: chunks of ~16k
+  // sites ran faster per step than whole 32k-site windows, by more than their
+  // burn-ins cost (the chromosome job, 32,768-site cores: whole 179.0 ms,
+  // two chunks 174.9, three 179-186, four 182.4).
+  if (tasks >= 2 * resident_tiles)
+    return ctx->spec_max_chunk > 0
+               ? (int)std::min<int64_t>(k_max, ceil_div(core_len, ctx->spec_max_chunk))
+               : 1;
   auto tiles_for = [&](int K) {
     if (slot_budget <= 0.0 || row_bytes <= 0.0) return resident_tiles;
     const double fit = slot_budget / ((double)ceil_div(core_len, K) * row_bytes);
@@ -830,6 +839,7 @@ bool summary_by_pairs(const gsmc_ctx* ctx, int64_t P, const std::vector<Block>& 
   const ScanShape one{scan_threads(), 1};
   const int64_t tasks = (int64_t)blocks.size() * ceil_div(P, scan_tile_pairs(one));
   const int64_t resident_tiles = (int64_t)resident_ctas(one) * scan_tiles_per_cta(one);
+  if (tasks >= 2 * resident_tiles) return false;  // the plain tasks fill the GPU
   return spec_chunks(ctx, tasks, resident_tiles, max_core(blocks), 0) > 1;
 }
 

@@ -24,7 +24,7 @@ CUDA_SOURCES = ["scan.cu", "capi.cu", "hostcopy.cu", "exec.cu", "fwd.cu", "flowg
                 "noalloc.cu", "tables_gpu.cu"]
 CXX_SOURCES = ["tables.cpp"]
 HEADERS = ["scan.h", "scan_device.cuh", "tables.h", "hostcopy.h", "ctx_view.h", "fwd.h", "flowgen.h", "uncached.h",
-           "windows.h", "tables_gpu.h"]
+           "windows.h", "tables_gpu.h", "planner.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",

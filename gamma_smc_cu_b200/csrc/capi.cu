@@ -27,6 +27,7 @@
 #include "tables.h"
 #include "tables_gpu.h"
 #include "uncached.h"
+#include "planner.h"
 #include "windows.h"
 
 using namespace gsmc;
@@ -429,8 +430,14 @@ int resident_ctas(ScanShape shape) {
 
 int spec_chunks(const gsmc_ctx* ctx, int64_t tasks, int64_t resident_tiles, int64_t core_len,
                 int flags, double row_bytes = 0.0, double slot_budget = 0.0);
-double launch_cost(int64_t n, int64_t r, double steps);
-double chunk_steps(int64_t core_len, int K, int64_t b, double w);
+plan::ChunkPolicy chunk_policy(const gsmc_ctx* ctx) {
+  plan::ChunkPolicy p;
+  p.burn_in = ctx->spec_flank;
+  p.max_chunk = ctx->spec_max_chunk;
+  return p;
+}
+using plan::chunk_steps;
+using plan::launch_cost;
 int64_t max_core(const std::vector<Block>& blocks);
 
 // Launch shape of a call over P pairs x `blocks`: two pairs per thread (two
@@ -599,31 +606,6 @@ struct SpecLaunch {
   int64_t max_core = 0;             // longest whole core (repair slot rows)
 };
 
-// Estimated duration, in pair-steps of one tile, of a persistent launch of n
-// equal tasks of `steps` pair-steps each on r resident tiles: full waves of r
-// tasks plus a partial wave of fraction f.  A partial wave runs faster than
-// its share of the GPU (fewer CTAs share the SMs) and, after full waves,
-// overlaps their uneven ends; fitted on the 50,000-site full-posterior slice
-// (63,190 pairs, 1,184 resident tiles, 2 to 8 chunks): alone it costs
-// 0.3 + 0.64 f of a full wave, after full waves 0.26 + 0.37 f.
-double launch_cost(int64_t n, int64_t r, double steps) {
-  if (n <= 0 || r <= 0) return 0.0;
-  const int64_t full = n / r;
-  const double f = (double)(n % r) / (double)r;
-  const double part = f <= 0.0 ? 0.0 : (full == 0 ? 0.3 + 0.64 * f : 0.26 + 0.37 * f);
-  return steps * ((double)full + part);
-}
-
-// Longest task (burn-in-step units per pair) of a core of core_len sites cut
-// into K chunks with burn-in b, cut as chunk_cuts does (no window flanks):
-// each interior boundary adds b forward steps to the right chunk and b
-// backward steps to the left one, a core site costs w, and the cuts share the
-// cost out evenly.
-double chunk_steps(int64_t core_len, int K, int64_t b, double w) {
-  if (K <= 1) return 2.0 * w * (double)core_len;
-  return (2.0 * w * (double)core_len + 2.0 * (K - 1) * (double)b) / K;
-}
-
 // Cut points of window b's core into K speculative chunks of equal cost
 // (chunk_cuts in windows.h).
 std::vector<int64_t> chunk_cuts(const Block& b, int K, int64_t flank, double w) {
@@ -640,54 +622,15 @@ int64_t longest_chunk(const Block& b, int K, int64_t flank, double w) {
   return m;
 }
 
-// Chunks per window for a launch of `tasks` tasks on `resident_tiles`
-// tiles: when the tasks fill the GPU twice, only as many as keep chunks
-// within the chunk cap; otherwise the K (chunks of
-// at least two burn-ins) that minimises launch_cost -- balancing the
-// burn-in steps each extra chunk adds against filling the last wave.  With
-// a slot budget, a tile's forward-state slot holds ceil(core / K) rows of
-// `row_bytes`, and only the tiles whose slots fit the budget run at once.
+// Chunks per window for a launch of `tasks` tasks on `resident_tiles` tiles
+// (plan::choose_chunks), unless speculation is off, fixed, or a summary.
 int spec_chunks(const gsmc_ctx* ctx, int64_t tasks, int64_t resident_tiles, int64_t core_len,
                 int flags, double row_bytes, double slot_budget) {
   if (!ctx->speculate || (flags & kTaskSummary) || tasks <= 0) return 1;
   if (ctx->spec_chunks_fixed > 0)
     return (int)std::max<int64_t>(1, std::min<int64_t>(ctx->spec_chunks_fixed, core_len / 64));
-  const int64_t b = ctx->spec_flank;
-  const int k_max = (int)std::max<int64_t>(1, std::min<int64_t>(1024, core_len / (2 * b)));
-  // Launches that fill the GPU twice over need no chunks to fill it, but
-  // windows longer than the chunk cap are still cut to it: chunks of ~16k
-  // sites ran faster per step than whole 32k-site windows, by more than their
-  // burn-ins cost (the chromosome job, 32,768-site cores: whole 179.0 ms,
-  // two chunks 174.9, three 179-186, four 182.4).
-  if (tasks >= 2 * resident_tiles)
-    return ctx->spec_max_chunk > 0
-               ? (int)std::min<int64_t>(k_max, ceil_div(core_len, ctx->spec_max_chunk))
-               : 1;
-  auto tiles_for = [&](int K) {
-    if (slot_budget <= 0.0 || row_bytes <= 0.0) return resident_tiles;
-    const double fit = slot_budget / ((double)ceil_div(core_len, K) * row_bytes);
-    return std::max<int64_t>(1, std::min<int64_t>(resident_tiles, (int64_t)fit));
-  };
-  // Once a window is cut, its chunks are kept short: with the same waves,
-  // chunks of 15-17k sites ran faster than 33k-site ones (the per-site
-  // summary's 23,600-pair batches over 400,000 sites: 0.25 s at 27 chunks,
-  // 0.32 s at 12), as did the slice's 12.5k-site chunks.
-  const int k_min = ctx->spec_max_chunk > 0
-                        ? (int)std::min<int64_t>(k_max, ceil_div(core_len, ctx->spec_max_chunk))
-                        : 1;
-  // Near-ties go to the fewest chunks (fewest burn-ins and boundaries to
-  // verify): within 1% of the cheapest.  (The slice: K = 4 at 1.002 of K = 9,
-  // measured 31.7 ms against 33.0 at K = 8.  A wider 5% let 8,192 pairs x
-  // 50,000 sites take K = 11 at 1.024 of K = 12: 7.45 ms against 6.86.)
-  std::vector<double> cost(k_max + 1, 1e300);
-  double lowest = 1e300;
-  for (int K = k_min; K <= k_max; ++K) {
-    cost[K] = launch_cost(tasks * K, tiles_for(K), chunk_steps(core_len, K, b, 1.0));
-    lowest = std::min(lowest, cost[K]);
-  }
-  for (int K = k_min; K <= k_max; ++K)
-    if (cost[K] <= 1.01 * lowest) return K;
-  return k_min;
+  return plan::choose_chunks(chunk_policy(ctx), tasks, resident_tiles, core_len, row_bytes,
+                             slot_budget);
 }
 
 // Append the tasks of window b for the n pairs at (pi, pj): whole, or in K
@@ -798,25 +741,10 @@ int run_direct(gsmc_ctx* ctx, const int32_t* d_pi, const int32_t* d_pj, int64_t 
   for (size_t i = 0; i < blocks.size(); ++i)
     K[i] = spec_chunks(ctx, plain_tasks, resident_tiles, blocks[i].ce - blocks[i].cs, flags,
                        (double)tile * sizeof(float2), (double)budget);
-  // A launch of several waves ends with the tasks that start last running on
-  // a partly empty GPU.  When its last wave is small (under a quarter of the
-  // resident tiles), one more window is cut in twice as many chunks, so the
-  // launch ends on half-length tasks: the chromosome job 174.0 -> 169.8 and
-  // 176.1 -> 173.6 ms on two boxes (two windows, or one cut in four, gained
-  // less).
-  if (ctx->speculate && ctx->spec_chunks_fixed == 0 && plain_tasks >= 2 * resident_tiles &&
-      !(flags & kTaskSummary)) {
-    int64_t n = 0;
-    for (size_t i = 0; i < blocks.size(); ++i) n += ceil_div(P, tile) * K[i];
-    const int64_t last_wave = n % resident_tiles;
-    if (last_wave > 0 && last_wave < resident_tiles / 4) {
-      for (size_t i = 0; i < blocks.size(); ++i) {
-        if (2 * K[i] <= (blocks[i].ce - blocks[i].cs) / (2 * ctx->spec_flank)) {
-          K[i] *= 2;
-          break;
-        }
-      }
-    }
+  if (ctx->speculate && ctx->spec_chunks_fixed == 0 && !(flags & kTaskSummary)) {
+    std::vector<int64_t> core(blocks.size());
+    for (size_t i = 0; i < blocks.size(); ++i) core[i] = blocks[i].ce - blocks[i].cs;
+    plan::split_tail(chunk_policy(ctx), ceil_div(P, tile), resident_tiles, core, &K);
   }
   for (size_t i = 0; i < blocks.size(); ++i) n_bnd += K[i] - 1;
   int rc = spec_reserve(ctx, n_bnd, P);

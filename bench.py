@@ -479,7 +479,7 @@ def timed_device_run(ctx, d_pi, d_pj, P, S, core, flank, flags, outs, steps, war
 
 
 def run_full_posterior(G, pos, pairs, steps, warmup, dev, n_sites=50_000):
-    """North-star roofline case: mean + posterior alpha/beta (12.25 B per
+    """Full-posterior roofline case: mean + posterior alpha/beta (12.25 B per
     pair-site) on the first 50,000 sites of the chromosome cohort, all pairs,
     blockwise with the API's auto core and flank 2048, outputs in HBM."""
     import torch

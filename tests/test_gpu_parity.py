@@ -1,7 +1,7 @@
 """Parity of the CUDA path with the oracle (and with the reference's compiled
 code when oracle/_ref holds it), through the C ABI.
 
-Tolerance: the north-star bar is 1e-4 relative on the posterior mean; the
+Tolerance: 1e-4 relative on the posterior mean is the bar for this path; the
 kernels are written to be bit-identical, which the *_bit_exact tests check.
 """
 import ctypes

@@ -1,6 +1,7 @@
 // C ABI of the B200 Gamma-SMC scan: contexts, table sets, window planning and
 // the host/device entry points declared in include/gsmc_b200.h.
 #include <cuda_runtime.h>
+#include <sys/mman.h>
 
 #include <algorithm>
 #include <atomic>
@@ -45,27 +46,68 @@ thread_local FlowFbStats g_flow_fb_stats;
 
 // Page-locked result buffers (gsmc_host_alloc): blocks in use, and released
 // blocks kept for reuse (up to g_host_cache_cap bytes), oldest first.
+struct HostBlk {
+  void* p;
+  uint64_t bytes;  // usable bytes (a mapped block: the whole mapping)
+  bool mapped;     // an anonymous mapping registered with CUDA, else cudaHostAlloc
+};
 std::mutex g_host_mu;
-std::map<void*, uint64_t> g_host_used;
-std::vector<std::pair<void*, uint64_t>> g_host_free;
+std::map<void*, HostBlk> g_host_used;
+std::vector<HostBlk> g_host_free;
 uint64_t g_host_cached = 0;
 uint64_t g_host_cache_cap = uint64_t(256) << 30;
+
+// Blocks of at least this many bytes are anonymous mappings advised
+// MADV_HUGEPAGE, page-locked with cudaHostRegister: on a B200 host that
+// page-locked 16 GB in 2.0 s against 6.5 s for cudaHostAlloc (4 KB pages
+// registered: 4.8 s).
+constexpr uint64_t kMappedMin = uint64_t(64) << 20;
+constexpr uint64_t kHugePage = uint64_t(2) << 20;
+
+// A new page-locked block of at least `bytes`.
+cudaError_t new_host_block(uint64_t bytes, HostBlk* out) {
+  if (bytes >= kMappedMin) {
+    const uint64_t size = (bytes + kHugePage - 1) / kHugePage * kHugePage;
+    void* p = mmap(nullptr, size, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
+    if (p != MAP_FAILED) {
+      madvise(p, size, MADV_HUGEPAGE);  // advice only: ignored where unsupported
+      const cudaError_t e = cudaHostRegister(p, size, cudaHostRegisterPortable);
+      if (e == cudaSuccess) {
+        *out = HostBlk{p, size, true};
+        return cudaSuccess;
+      }
+      munmap(p, size);
+      return e;
+    }
+  }
+  void* p = nullptr;
+  const cudaError_t e = cudaHostAlloc(&p, bytes, cudaHostAllocPortable);
+  if (e == cudaSuccess) *out = HostBlk{p, bytes, false};
+  return e;
+}
 
 // Take cached blocks out until the cache is within its cap; the caller frees
 // them with free_host_blocks after releasing g_host_mu (unpinning a large
 // block takes seconds, and other threads' allocations must not wait on it).
-std::vector<std::pair<void*, uint64_t>> trim_host_cache_locked() {
-  std::vector<std::pair<void*, uint64_t>> out;
+std::vector<HostBlk> trim_host_cache_locked() {
+  std::vector<HostBlk> out;
   while (g_host_cached > g_host_cache_cap && !g_host_free.empty()) {
     out.push_back(g_host_free.front());
-    g_host_cached -= g_host_free.front().second;
+    g_host_cached -= g_host_free.front().bytes;
     g_host_free.erase(g_host_free.begin());
   }
   return out;
 }
 
-void free_host_blocks(const std::vector<std::pair<void*, uint64_t>>& blocks) {
-  for (const auto& kv : blocks) cudaFreeHost(kv.first);
+void free_host_blocks(const std::vector<HostBlk>& blocks) {
+  for (const HostBlk& b : blocks) {
+    if (b.mapped) {
+      cudaHostUnregister(b.p);
+      munmap(b.p, b.bytes);
+    } else {
+      cudaFreeHost(b.p);
+    }
+  }
 }
 
 // mbarrier polls the uncached kernels wait for their flow-field copy.
@@ -1916,24 +1958,24 @@ int gsmc_host_alloc(uint64_t bytes, void** ptr) {
     // the smallest cached block that fits without wasting more than half of it
     auto best = g_host_free.end();
     for (auto it = g_host_free.begin(); it != g_host_free.end(); ++it)
-      if (it->second >= bytes && it->second / 2 <= bytes &&
-          (best == g_host_free.end() || it->second < best->second))
+      if (it->bytes >= bytes && it->bytes / 2 <= bytes &&
+          (best == g_host_free.end() || it->bytes < best->bytes))
         best = it;
     if (best != g_host_free.end()) {
-      *ptr = best->first;
-      g_host_used[best->first] = best->second;
-      g_host_cached -= best->second;
+      *ptr = best->p;
+      g_host_used[best->p] = *best;
+      g_host_cached -= best->bytes;
       g_host_free.erase(best);
       return GSMC_OK;
     }
   }
   // Page-locking runs outside the lock: it takes seconds for tens of GB.
-  void* p = nullptr;
-  cudaError_t e = cudaHostAlloc(&p, bytes, cudaHostAllocPortable);
+  HostBlk blk{};
+  cudaError_t e = new_host_block(bytes, &blk);
   if (e != cudaSuccess) {
     // release the cache and try once more
     cudaGetLastError();
-    std::vector<std::pair<void*, uint64_t>> drop;
+    std::vector<HostBlk> drop;
     {
       std::lock_guard<std::mutex> lock(g_host_mu);
       drop.swap(g_host_free);
@@ -1941,7 +1983,7 @@ int gsmc_host_alloc(uint64_t bytes, void** ptr) {
     }
     if (!drop.empty()) {
       free_host_blocks(drop);
-      e = cudaHostAlloc(&p, bytes, cudaHostAllocPortable);
+      e = new_host_block(bytes, &blk);
     }
   }
   if (e != cudaSuccess) {
@@ -1951,21 +1993,21 @@ int gsmc_host_alloc(uint64_t bytes, void** ptr) {
   }
   {
     std::lock_guard<std::mutex> lock(g_host_mu);
-    g_host_used[p] = bytes;
+    g_host_used[blk.p] = blk;
   }
-  *ptr = p;
+  *ptr = blk.p;
   return GSMC_OK;
 }
 
 int gsmc_host_free(void* ptr) {
   if (!ptr) return GSMC_OK;
-  std::vector<std::pair<void*, uint64_t>> drop;
+  std::vector<HostBlk> drop;
   {
     std::lock_guard<std::mutex> lock(g_host_mu);
     auto it = g_host_used.find(ptr);
     if (it == g_host_used.end()) return fail(GSMC_E_INVALID, "not a gsmc_host_alloc buffer");
-    g_host_free.emplace_back(it->first, it->second);
-    g_host_cached += it->second;
+    g_host_free.push_back(it->second);
+    g_host_cached += it->second.bytes;
     g_host_used.erase(it);
     drop = trim_host_cache_locked();
   }
@@ -1974,7 +2016,7 @@ int gsmc_host_free(void* ptr) {
 }
 
 int gsmc_host_cache_limit(uint64_t max_cached_bytes) {
-  std::vector<std::pair<void*, uint64_t>> drop;
+  std::vector<HostBlk> drop;
   {
     std::lock_guard<std::mutex> lock(g_host_mu);
     g_host_cache_cap = max_cached_bytes;

@@ -446,9 +446,12 @@ int gsmc_free_cached_tables(void);
  * Page-locked host buffers for results, cached for reuse.  A host output
  * array that is page-locked is written by the device-to-host DMA directly
  * (no staging ring, no host thread touching the data), which is what repeated
- * large calls want; allocating page-locked memory is slow (seconds per 100
- * GB), so released buffers are kept and handed out again to requests they fit
- * (at most twice the request).  gsmc_host_free returns a buffer to the cache;
+ * large calls want; page-locking is slow (seconds per 10 GB), so released
+ * buffers are kept and handed out again to requests they fit (at most twice
+ * the request).  Buffers of 64 MB or more are anonymous mappings of whole
+ * 2 MB pages advised MADV_HUGEPAGE and registered with cudaHostRegister
+ * (about three times faster to page-lock than cudaHostAlloc's memory);
+ * smaller ones come from cudaHostAlloc.  gsmc_host_free returns a buffer to the cache;
  * gsmc_host_cache_limit bounds the bytes kept cached (default 256 GiB;
  * 0 frees every cached buffer).  No reference counterpart (the reference
  * pins its fresh output arrays with cudaHostRegister on every call,

@@ -1226,7 +1226,7 @@ def run_e2e(G, pos, pairs, core, flank, steps):
 #   batch     64 uneven jobs (1-2,000 pairs, 2k-40k-site windows) over a
 #             60,000-site slice, one executor launch (32-thread tiles,
 #             4,096-site chunks)
-#   summary   per-site summary, 16,384 pairs x 20,000 sites (8,192 / 2,048)
+#   summary   per-site summary, all 63,190 pairs x 20,000 sites (2,048 / 1,024)
 #   fwd       forward-only posterior, 8,192 pairs x 20,000 sites
 #   uncached  uncached flow-field FB, 4,096 pairs x 10,000 sites
 #   flowgen   GPU flow-field generation, 51 x 50 cells, constant Ne
@@ -1325,10 +1325,13 @@ def case_batch(repeat):
 
 def case_summary(repeat):
     from gamma_smc_cu_b200 import synthetic
+    # enough (window, pair tile) tasks to fill the GPU twice, so the call runs
+    # the summary instantiation itself (fewer go through per-pair means in
+    # speculative chunks)
     ctx, G, pos = _case_ctx(20000)
-    pairs = synthetic.random_pairs(G.shape[0], 16384, 3)
+    pairs = synthetic.all_pairs(G.shape[0])
     for _ in range(1 + repeat):
-        ctx.run_fb_summary(pairs, core_block_sites=8192, flank_sites=2048)
+        ctx.run_fb_summary(pairs, core_block_sites=2048, flank_sites=1024)
 
 
 def case_fwd(repeat):

@@ -1297,6 +1297,9 @@ int gsmc_run_fb_summary(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pai
     int64_t batch = std::max<int64_t>(1, (int64_t)(0.3 * (double)budget / (double)(S * 4)));
     batch = std::min(batch, n_pairs);
     if (pair_batch_size > 0) batch = std::min(batch, pair_batch_size);
+    // equal batches: a small last one would run its long windows on a mostly
+    // idle GPU (63,190 pairs in batches of 28,775 left 5,640 for the last)
+    batch = ceil_div(n_pairs, ceil_div(n_pairs, batch));
     rc = ensure_buffer(&ctx->stage, &ctx->stage_bytes, (size_t)S * batch * sizeof(float));
     if (rc) return rc;
     for (int64_t off = 0; off < n_pairs; off += batch) {
@@ -1327,6 +1330,10 @@ int gsmc_run_fb_summary(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pai
   chunk_tiles = std::min<int64_t>(chunk_tiles, ceil_div(n_pairs, tile));
   if (pair_batch_size > 0)
     chunk_tiles = std::min<int64_t>(chunk_tiles, std::max<int64_t>(1, pair_batch_size / tile));
+  {  // equal pair chunks (no small last one)
+    const int64_t all_tiles = ceil_div(n_pairs, tile);
+    chunk_tiles = ceil_div(all_tiles, ceil_div(all_tiles, chunk_tiles));
+  }
   const int64_t chunk = chunk_tiles * tile;
   const int64_t cols = chunk_tiles * warps;
   rc = ensure_buffer(&ctx->stage, &ctx->stage_bytes, (size_t)3 * S * cols * sizeof(float));

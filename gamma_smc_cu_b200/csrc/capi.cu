@@ -866,6 +866,7 @@ int run_to_host(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int6
     if (need <= budget || chunk <= tile) break;
     chunk = std::max<int64_t>(tile, chunk / 2);
   }
+  chunk = ceil_div(P, ceil_div(P, chunk));  // equal pair chunks, no small last one
   const size_t half = (size_t)group * core * chunk * nout;  // floats per stage half
   int rc = ensure_buffer(&ctx->stage, &ctx->stage_bytes, 2 * half * sizeof(float));
   if (rc) return rc;

@@ -1818,7 +1818,11 @@ int gsmc_flow_fb(const uint8_t* G, int64_t n_haps, int64_t n_sites, const double
   const size_t per_pair = (size_t)n_sites * (8 + 4 * nout);
   const size_t budget = (size_t)(0.6 * (double)free_device_bytes());
   int64_t chunk = std::min<int64_t>(n_pairs, std::max<int64_t>(1, (int64_t)(budget / per_pair)));
-  if (chunk < n_pairs) chunk = std::max<int64_t>(256, chunk / 256 * 256);
+  if (chunk < n_pairs) {
+    chunk = std::max<int64_t>(256, chunk / 256 * 256);
+    // equal chunks (multiples of 256, none larger than the budget's)
+    chunk = std::min(chunk, ceil_div(ceil_div(n_pairs, ceil_div(n_pairs, chunk)), 256) * 256);
+  }
   struct Bufs {
     uint8_t* G = nullptr;
     ulonglong2* geno = nullptr;

@@ -1159,7 +1159,21 @@ def run_e2e(G, pos, pairs, core, flank, steps):
         ctx.close()
         return r, info, t_ctx
 
+    def infer_once():
+        # the reference's own public entry point on the same inputs: input
+        # checks, segregating-site filter, theta estimate on the GPU, context,
+        # decode, results
+        from gamma_smc_cu_b200.infer import infer_blockwise
+        t0 = time.perf_counter()
+        r = infer_blockwise(Gs, ps, pairs=plist, core_block_sites=core, flank_sites=flank,
+                            pair_batch_size=P, mean_only=True)
+        dt = time.perf_counter() - t0
+        log(f"e2e through infer_blockwise {dt:.2f} s")
+        del r
+        return dt
+
     memory = "page-locked buffers reused across calls"
+    api_s = None
     prev = _core.set_result_memory("pinned")
     try:
         t0 = time.perf_counter()
@@ -1175,6 +1189,7 @@ def run_e2e(G, pos, pairs, core, flank, steps):
             ctx_s.append(t_ctx)
             log(f"e2e step {times[-1]:.2f} s")
             del r
+        api_s = infer_once()
     except MemoryError as e:   # the host could not page-lock the results
         memory = f"pageable numpy arrays (page-locking failed: {e})"
         times = None
@@ -1207,7 +1222,8 @@ def run_e2e(G, pos, pairs, core, flank, steps):
             "first_call_seconds": first_s,
             "table_build_seconds_first_call": info0["build_seconds"],
             "tables_reused_in_timed_steps": bool(info["reused"]),
-            "pageable_seconds": pageable_s, "pageable_value": P * sites / pageable_s}
+            "pageable_seconds": pageable_s, "pageable_value": P * sites / pageable_s,
+            "infer_blockwise_seconds": api_s}
 
 
 # ------------------------------------------------------------ profiling cases

@@ -866,7 +866,7 @@ int run_to_host(gsmc_ctx* ctx, int64_t P, const std::vector<Block>& blocks, int6
     if (need <= budget || chunk <= tile) break;
     chunk = std::max<int64_t>(tile, chunk / 2);
   }
-  chunk = ceil_div(P, ceil_div(P, chunk));  // equal pair chunks, no small last one
+  chunk = plan::even_part(P, chunk);  // equal pair chunks, no small last one
   const size_t half = (size_t)group * core * chunk * nout;  // floats per stage half
   int rc = ensure_buffer(&ctx->stage, &ctx->stage_bytes, 2 * half * sizeof(float));
   if (rc) return rc;
@@ -1300,7 +1300,7 @@ int gsmc_run_fb_summary(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pai
     if (pair_batch_size > 0) batch = std::min(batch, pair_batch_size);
     // equal batches: a small last one would run its long windows on a mostly
     // idle GPU (63,190 pairs in batches of 28,775 left 5,640 for the last)
-    batch = ceil_div(n_pairs, ceil_div(n_pairs, batch));
+    batch = plan::even_part(n_pairs, batch);
     rc = ensure_buffer(&ctx->stage, &ctx->stage_bytes, (size_t)S * batch * sizeof(float));
     if (rc) return rc;
     for (int64_t off = 0; off < n_pairs; off += batch) {
@@ -1333,7 +1333,7 @@ int gsmc_run_fb_summary(gsmc_ctx* ctx, const int32_t* pair_i, const int32_t* pai
     chunk_tiles = std::min<int64_t>(chunk_tiles, std::max<int64_t>(1, pair_batch_size / tile));
   {  // equal pair chunks (no small last one)
     const int64_t all_tiles = ceil_div(n_pairs, tile);
-    chunk_tiles = ceil_div(all_tiles, ceil_div(all_tiles, chunk_tiles));
+    chunk_tiles = plan::even_part(all_tiles, chunk_tiles);
   }
   const int64_t chunk = chunk_tiles * tile;
   const int64_t cols = chunk_tiles * warps;
@@ -1821,7 +1821,7 @@ int gsmc_flow_fb(const uint8_t* G, int64_t n_haps, int64_t n_sites, const double
   if (chunk < n_pairs) {
     chunk = std::max<int64_t>(256, chunk / 256 * 256);
     // equal chunks (multiples of 256, none larger than the budget's)
-    chunk = std::min(chunk, ceil_div(ceil_div(n_pairs, ceil_div(n_pairs, chunk)), 256) * 256);
+    chunk = plan::even_part(n_pairs, chunk, 256);
   }
   struct Bufs {
     uint8_t* G = nullptr;

@@ -41,6 +41,20 @@ inline double chunk_steps(int64_t core_len, int K, int64_t b, double w) {
   return (2.0 * w * (double)core_len + 2.0 * (K - 1) * (double)b) / K;
 }
 
+// Size of the parts when n items are cut into as few parts of at most `cap`
+// as possible, made as equal as possible: ceil(n / ceil(n / cap)).  Pair
+// batches and pair chunks use it so no small last part runs on a mostly idle
+// GPU (the per-site summary: 28,775 + 28,775 + 5,640 pairs took 0.265 s,
+// three batches of 21,064 took 0.217 s).  With `multiple` > 1 the size is
+// rounded up to a multiple of it, never above `cap` when `cap` is one.
+inline int64_t even_part(int64_t n, int64_t cap, int64_t multiple = 1) {
+  if (n <= 0 || cap <= 0) return std::max<int64_t>(1, cap);
+  const int64_t part = cdiv(n, cdiv(n, cap));
+  if (multiple <= 1) return part;
+  return std::min<int64_t>(cap >= multiple ? cap : cdiv(cap, multiple) * multiple,
+                           cdiv(part, multiple) * multiple);
+}
+
 // What the chunk count depends on besides the launch.
 struct ChunkPolicy {
   int64_t burn_in = 2048;     // burn-in sites of a chunk

@@ -160,7 +160,10 @@ def _empty_huge(shape, n):
     # a whole number of 2 MB pages: the kernel places such mappings on a 2 MB
     # boundary, so every page of the array can be a huge one
     size = -(-4 * n // (2 << 20)) * (2 << 20)
-    m = mmap.mmap(-1, size, flags=mmap.MAP_PRIVATE | mmap.MAP_ANONYMOUS)
+    try:
+        m = mmap.mmap(-1, size, flags=mmap.MAP_PRIVATE | mmap.MAP_ANONYMOUS)
+    except (OSError, ValueError):   # no mapping: np.empty's memory (or its MemoryError)
+        return np.empty(shape, np.float32)
     try:
         m.madvise(mmap.MADV_HUGEPAGE)
     except (AttributeError, OSError, ValueError):

@@ -44,3 +44,16 @@ def test_small_results_and_switch(monkeypatch):
     assert big.base is None and big.dtype == np.float32
     empty = _core._empty((0, 5))
     assert empty.shape == (0, 5)
+
+
+def test_mapping_failure_falls_back_to_np_empty(monkeypatch):
+    import mmap
+
+    def refuse(*a, **k):
+        raise OSError(12, "Cannot allocate memory")
+
+    monkeypatch.setattr(_core, "_HUGEPAGES", True)
+    monkeypatch.setattr(_core, "_RESULT_MEMORY", "pageable")
+    monkeypatch.setattr(mmap, "mmap", refuse)
+    a = _core._empty((1000, 17_000))
+    assert a.base is None and a.shape == (1000, 17_000) and a.dtype == np.float32
